@@ -1,0 +1,83 @@
+"""Build recipe of the B200 solver library and its command-line programs.
+
+Compiles, for sm_100a only:
+  lib/libgpe.so            C ABI (include/gpe.h): kernels + handle
+  bin/imag3d-mpicuda       drop-in CLI for imaginary time
+  bin/real3d-mpicuda       drop-in CLI for real time
+Uses nvcc directly (no torch extension): the library has no torch types in
+its interface.  Outputs stay inside the package directory so they travel with
+the repository snapshot.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+HOST = os.path.join(PKG, "host")
+LIB_DIR = os.path.join(PKG, "lib")
+BIN_DIR = os.path.join(PKG, "bin")
+INCLUDE = os.path.join(ROOT, "include")
+
+NVCC = os.environ.get("NVCC", "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
+                  "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC]
+
+LIB_SOURCES = ["solver.cu"]
+LIB_DEPS = ["solver.cu", "common.cuh", "fft.cuh", "kernels.cuh", "step_kernels.cuh"]
+HOST_COMMON = ["cfg.cpp", "cli.cpp"]
+PROGRAMS = {"imag3d-mpicuda": "imag3d_main.cpp", "real3d-mpicuda": "real3d_main.cpp"}
+
+LIB = os.path.join(LIB_DIR, "libgpe.so")
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def _run(cmd):
+    print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def build_lib(force=False, verbose_ptxas=False):
+    os.makedirs(LIB_DIR, exist_ok=True)
+    deps = [os.path.join(CSRC, f) for f in LIB_DEPS] + [os.path.join(INCLUDE, "gpe.h")]
+    if force or _stale(LIB, deps):
+        extra = ["-Xptxas", "-v"] if verbose_ptxas else []
+        _run([NVCC] + NVFLAGS + extra + ["-shared", "-o", LIB] +
+             [os.path.join(CSRC, f) for f in LIB_SOURCES] + ["-lcudart"])
+    return LIB
+
+
+def build_programs(force=False):
+    os.makedirs(BIN_DIR, exist_ok=True)
+    out = {}
+    common = [os.path.join(HOST, f) for f in HOST_COMMON]
+    for name, main in PROGRAMS.items():
+        target = os.path.join(BIN_DIR, name)
+        srcs = common + [os.path.join(HOST, main)]
+        deps = srcs + [os.path.join(HOST, "cfg.h"), os.path.join(HOST, "cli.h"), LIB]
+        if force or _stale(target, deps):
+            _run(["g++", "-O2", "-std=c++17", "-I" + INCLUDE, "-I" + HOST, "-o", target] + srcs +
+                 ["-L" + LIB_DIR, "-lgpe", "-Wl,-rpath,$ORIGIN/../lib"])
+        out[name] = target
+    return out
+
+
+def build(force=False):
+    build_lib(force)
+    if os.path.exists(os.path.join(HOST, "cli.cpp")):
+        build_programs(force)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv)

@@ -1,0 +1,101 @@
+// common.cuh -- element types, complex helpers and the Simpson accumulator
+// shared by every kernel of the B200 dipolar GP solver.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace gpe {
+
+template <class R> struct vec2;
+template <> struct vec2<double> { using type = double2; };
+template <> struct vec2<float> { using type = float2; };
+
+template <class R> using cpx = typename vec2<R>::type;
+
+template <class R> __host__ __device__ __forceinline__ cpx<R> mk(R x, R y) { cpx<R> r; r.x = x; r.y = y; return r; }
+template <class C> __host__ __device__ __forceinline__ C cadd(C a, C b) { C r; r.x = a.x + b.x; r.y = a.y + b.y; return r; }
+template <class C> __host__ __device__ __forceinline__ C csub(C a, C b) { C r; r.x = a.x - b.x; r.y = a.y - b.y; return r; }
+template <class C> __host__ __device__ __forceinline__ C cmul(C a, C b) {
+   C r; r.x = a.x * b.x - a.y * b.y; r.y = a.x * b.y + a.y * b.x; return r;
+}
+template <class C> __host__ __device__ __forceinline__ C cconj(C a) { C r; r.x = a.x; r.y = -a.y; return r; }
+template <class C, class S> __host__ __device__ __forceinline__ C cscale(C a, S s) { C r; r.x = a.x * s; r.y = a.y * s; return r; }
+// multiply by -i (forward) or +i (inverse)
+template <class C, bool INV> __host__ __device__ __forceinline__ C mul_mi(C a) {
+   C r;
+   if (INV) { r.x = -a.y; r.y = a.x; } else { r.x = a.y; r.y = -a.x; }
+   return r;
+}
+
+// generic add/sub over real and complex psi elements
+__host__ __device__ __forceinline__ double cadd_any(double a, double b) { return a + b; }
+__host__ __device__ __forceinline__ float cadd_any(float a, float b) { return a + b; }
+__host__ __device__ __forceinline__ double2 cadd_any(double2 a, double2 b) { return cadd(a, b); }
+__host__ __device__ __forceinline__ float2 cadd_any(float2 a, float2 b) { return cadd(a, b); }
+__host__ __device__ __forceinline__ double csub_any(double a, double b) { return a - b; }
+__host__ __device__ __forceinline__ float csub_any(float a, float b) { return a - b; }
+__host__ __device__ __forceinline__ double2 csub_any(double2 a, double2 b) { return csub(a, b); }
+__host__ __device__ __forceinline__ float2 csub_any(float2 a, float2 b) { return csub(a, b); }
+
+// psi element: real R in imaginary time, complex in real time
+template <class R, bool CPLX> struct psi_elem { using type = R; };
+template <class R> struct psi_elem<R, true> { using type = cpx<R>; };
+
+template <class R> __device__ __forceinline__ R dens(R v) { return v * v; }
+template <class R> __device__ __forceinline__ R dens(typename vec2<R>::type v) { return v.x * v.x + v.y * v.y; }
+__device__ __forceinline__ double dens2(double v) { return v * v; }
+__device__ __forceinline__ double dens2(double2 v) { return v.x * v.x + v.y * v.y; }
+__device__ __forceinline__ float dens2(float v) { return v * v; }
+__device__ __forceinline__ float dens2(float2 v) { return v.x * v.x + v.y * v.y; }
+
+__device__ __forceinline__ double scl(double v, double s) { return v * s; }
+__device__ __forceinline__ double2 scl(double2 v, double s) { return make_double2(v.x * s, v.y * s); }
+__device__ __forceinline__ float scl(float v, double s) { return (float) (v * s); }
+__device__ __forceinline__ float2 scl(float2 v, double s) { return make_float2((float) (v.x * s), (float) (v.y * s)); }
+
+template <class T> __device__ __forceinline__ T zero_of();
+template <> __device__ __forceinline__ double zero_of<double>() { return 0.; }
+template <> __device__ __forceinline__ float zero_of<float>() { return 0.f; }
+template <> __device__ __forceinline__ double2 zero_of<double2>() { return make_double2(0., 0.); }
+template <> __device__ __forceinline__ float2 zero_of<float2>() { return make_float2(0.f, 0.f); }
+
+// Composite Simpson rule accumulated while walking a line in index order,
+// with the reference's three partial sums and end correction
+// (src/utils/diffint.cu:37-66): odd samples (sumi), the even sample before
+// each odd one (sumj) and the even sample after it (sumk).
+struct Simpson {
+   double si, sj, sk, f1, f2, f3;  // f1 = f[N-1] candidate chain
+   long n;
+   __host__ __device__ __forceinline__ void init(long N) { si = sj = sk = f1 = f2 = f3 = 0.; n = N; }
+   __host__ __device__ __forceinline__ void add(long k, double f) {
+      if (k & 1) {
+         if (k < n - 1) si += f;
+      } else {
+         if (k < n - 2) sj += f;
+         if (k >= 2) sk += f;
+      }
+      f3 = f2; f2 = f1; f1 = f;
+   }
+   // after add() was called for k = 0..N-1 in order
+   __host__ __device__ __forceinline__ double finish(double h) const {
+      double sum = sj + 4. * si + sk;
+      if (n % 2 == 0) sum += (5. * f1 + 8. * f2 - f3) / 4.;
+      return sum * h / 3.;
+   }
+};
+
+// Simpson over an array in memory, the reference's loop verbatim in order.
+__host__ __device__ __forceinline__ double simpint_arr(double h, const double *f, long N, long st = 1) {
+   double sumi = 0., sumj = 0., sumk = 0.;
+   for (long c = 1; c < N - 1; c += 2) {
+      sumi += f[c * st];
+      sumj += f[(c - 1) * st];
+      sumk += f[(c + 1) * st];
+   }
+   double sum = sumj + 4. * sumi + sumk;
+   if (N % 2 == 0) sum += (5. * f[(N - 1) * st] + 8. * f[(N - 2) * st] - f[(N - 3) * st]) / 4.;
+   return sum * h / 3.;
+}
+
+}  // namespace gpe

@@ -1,0 +1,158 @@
+// fft.cuh -- shared-memory mixed-radix Stockham FFT used by every FFT pass
+// of the dipolar convolution (the reference calls cuFFT D2Z/Z2Z/Z2D here,
+// src/imag3d-mpicuda/imag3d-mpicuda.cu:1460-1510; this is a project-written
+// transform, not cuFFT's).
+//
+// A CTA transforms L lines of length n held in shared memory.  Element j of
+// line l lives at base[l * ls + j * es].  Each radix-r stage (autosort
+// Stockham, decimation in time) reads from one buffer and writes the other:
+//   j in [0, n/r), k = j mod Ns,  v[t] = src[j + t n/r] * W_n^(t k n/(Ns r))
+//   v = DFT_r(v),  dst[(j / Ns) Ns r + k + t Ns] = v[t],  Ns *= r
+// which leaves the result in natural order after the last stage.  The
+// twiddle table holds W_n^m = exp(-2 pi i m / n), m in [0, n), computed on
+// the host in long double; inverse transforms use conjugated twiddles and
+// are unnormalised (like cuFFT's CUFFT_INVERSE).
+#pragma once
+
+#include "common.cuh"
+
+namespace gpe {
+
+constexpr int kMaxStages = 16;
+
+struct FftPlan {
+   int n;
+   int nst;
+   int rad[kMaxStages];
+};
+
+// ---- small DFT kernels (constants are exact values of cos/sin) -------------
+template <class C, bool INV> __device__ __forceinline__ void dft2(C *v) {
+   C a = v[0], b = v[1];
+   v[0] = cadd(a, b);
+   v[1] = csub(a, b);
+}
+
+template <class C, bool INV> __device__ __forceinline__ void dft3(C *v) {
+   using R = decltype(v[0].x);
+   const R s3 = (R) 0.86602540378443864676;  // sin(2 pi / 3)
+   C a = v[0], t1 = cadd(v[1], v[2]), t2 = csub(v[1], v[2]);
+   C m = csub(a, cscale(t1, (R) 0.5));
+   C r = cscale(mul_mi<C, INV>(t2), s3);  // -i s3 t2 (forward)
+   v[0] = cadd(a, t1);
+   v[1] = cadd(m, r);
+   v[2] = csub(m, r);
+}
+
+template <class C, bool INV> __device__ __forceinline__ void dft4(C *v) {
+   C t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+   C t2 = cadd(v[1], v[3]), t3 = mul_mi<C, INV>(csub(v[1], v[3]));
+   v[0] = cadd(t0, t2);
+   v[2] = csub(t0, t2);
+   v[1] = cadd(t1, t3);
+   v[3] = csub(t1, t3);
+}
+
+template <class C, bool INV> __device__ __forceinline__ void dft5(C *v) {
+   using R = decltype(v[0].x);
+   const R c1 = (R) 0.30901699437494742410, c2 = (R) -0.80901699437494742410;
+   const R s1 = (R) 0.95105651629515357212, s2 = (R) 0.58778525229247312917;
+   C a0 = v[0];
+   C b1 = cadd(v[1], v[4]), b2 = cadd(v[2], v[3]);
+   C d1 = csub(v[1], v[4]), d2 = csub(v[2], v[3]);
+   C p1 = cadd(a0, cadd(cscale(b1, c1), cscale(b2, c2)));
+   C p2 = cadd(a0, cadd(cscale(b1, c2), cscale(b2, c1)));
+   C q1 = mul_mi<C, INV>(cadd(cscale(d1, s1), cscale(d2, s2)));
+   C q2 = mul_mi<C, INV>(csub(cscale(d1, s2), cscale(d2, s1)));
+   v[0] = cadd(a0, cadd(b1, b2));
+   v[1] = cadd(p1, q1);
+   v[4] = csub(p1, q1);
+   v[2] = cadd(p2, q2);
+   v[3] = csub(p2, q2);
+}
+
+template <class C, bool INV> __device__ __forceinline__ void dft8(C *v) {
+   using R = decltype(v[0].x);
+   const R h = (R) 0.70710678118654752440;  // 1/sqrt(2)
+   C e[4] = {v[0], v[2], v[4], v[6]};
+   C o[4] = {v[1], v[3], v[5], v[7]};
+   dft4<C, INV>(e);
+   dft4<C, INV>(o);
+   // o[k] *= W8^k (forward W8 = (1 - i)/sqrt2)
+   C w1, w3;
+   if (INV) {
+      w1.x = (o[1].x - o[1].y) * h; w1.y = (o[1].x + o[1].y) * h;     // (1+i)/sqrt2
+      w3.x = (-o[3].x - o[3].y) * h; w3.y = (o[3].x - o[3].y) * h;    // (-1+i)/sqrt2
+   } else {
+      w1.x = (o[1].x + o[1].y) * h; w1.y = (o[1].y - o[1].x) * h;     // (1-i)/sqrt2
+      w3.x = (-o[3].x + o[3].y) * h; w3.y = (-o[3].x - o[3].y) * h;   // (-1-i)/sqrt2
+   }
+   C w2 = mul_mi<C, INV>(o[2]);
+   v[0] = cadd(e[0], o[0]); v[4] = csub(e[0], o[0]);
+   v[1] = cadd(e[1], w1);   v[5] = csub(e[1], w1);
+   v[2] = cadd(e[2], w2);   v[6] = csub(e[2], w2);
+   v[3] = cadd(e[3], w3);   v[7] = csub(e[3], w3);
+}
+
+template <int R, class C, bool INV> __device__ __forceinline__ void dftr(C *v) {
+   if constexpr (R == 2) dft2<C, INV>(v);
+   else if constexpr (R == 3) dft3<C, INV>(v);
+   else if constexpr (R == 4) dft4<C, INV>(v);
+   else if constexpr (R == 5) dft5<C, INV>(v);
+   else dft8<C, INV>(v);
+}
+
+// One Stockham stage over L lines.  JFAST: consecutive threads take
+// consecutive j of one line (line-major layouts); otherwise consecutive
+// lines (interleaved layouts).
+template <int RAD, class C, bool INV, bool JFAST>
+__device__ __forceinline__ void fft_stage(const C *__restrict__ src, C *__restrict__ dst, int n, int L, int ls,
+                                          int es, int Ns, const C *__restrict__ tw) {
+   const int nr = n / RAD;
+   const int nb = nr * L;
+   const int twstep = n / (Ns * RAD);
+   for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+      int j, l;
+      if (JFAST) { j = b % nr; l = b / nr; } else { l = b % L; j = b / L; }
+      const int k = j % Ns;
+      C v[RAD];
+      const C *s = src + l * ls + j * es;
+#pragma unroll
+      for (int t = 0; t < RAD; t++) v[t] = s[t * nr * es];
+      if (Ns > 1) {
+#pragma unroll
+         for (int t = 1; t < RAD; t++) {
+            C w = tw[t * k * twstep];
+            if (INV) w.y = -w.y;
+            v[t] = cmul(v[t], w);
+         }
+      }
+      dftr<RAD, C, INV>(v);
+      C *d = dst + l * ls + ((j / Ns) * Ns * RAD + k) * es;
+#pragma unroll
+      for (int t = 0; t < RAD; t++) d[t * Ns * es] = v[t];
+   }
+}
+
+// Full transform; returns the buffer (a or b) that holds the result.
+// All threads of the CTA must call it; it synchronises between stages.
+template <class C, bool INV, bool JFAST>
+__device__ C *fft_lines(C *a, C *b, const FftPlan &pl, int L, int ls, int es, const C *tw) {
+   int Ns = 1;
+   for (int st = 0; st < pl.nst; st++) {
+      const int r = pl.rad[st];
+      switch (r) {
+      case 2: fft_stage<2, C, INV, JFAST>(a, b, pl.n, L, ls, es, Ns, tw); break;
+      case 3: fft_stage<3, C, INV, JFAST>(a, b, pl.n, L, ls, es, Ns, tw); break;
+      case 4: fft_stage<4, C, INV, JFAST>(a, b, pl.n, L, ls, es, Ns, tw); break;
+      case 5: fft_stage<5, C, INV, JFAST>(a, b, pl.n, L, ls, es, Ns, tw); break;
+      default: fft_stage<8, C, INV, JFAST>(a, b, pl.n, L, ls, es, Ns, tw); break;
+      }
+      __syncthreads();
+      C *t = a; a = b; b = t;
+      Ns *= r;
+   }
+   return a;
+}
+
+}  // namespace gpe

@@ -1,0 +1,968 @@
+// solver.cu -- handle, tables and the C ABI (include/gpe.h) of the B200
+// dipolar Gross-Pitaevskii solver.  Host code only orchestrates; every
+// operator on psi runs in the kernels of step_kernels.cuh.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "gpe.h"
+#include "step_kernels.cuh"
+
+using namespace gpe;
+
+// The reference's truncated pi (imag3d-mpicuda.cu:69).
+static const double kRefPi = 3.14159265358979;
+
+static thread_local std::string g_err;
+
+static gpe_status fail(gpe_status st, const std::string &msg) {
+   g_err = msg;
+   return st;
+}
+
+#define CK(call)                                                                                   \
+   do {                                                                                           \
+      cudaError_t e_ = (call);                                                                    \
+      if (e_ != cudaSuccess)                                                                      \
+         return fail(e_ == cudaErrorMemoryAllocation ? GPE_ERR_OOM : GPE_ERR_CUDA,                \
+                     std::string(#call) + ": " + cudaGetErrorString(e_));                          \
+   } while (0)
+
+#define CKL()                                                                                      \
+   do {                                                                                           \
+      cudaError_t e_ = cudaGetLastError();                                                        \
+      if (e_ != cudaSuccess) return fail(GPE_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e_)); \
+   } while (0)
+
+#define CKS(expr)                                                                                  \
+   do {                                                                                           \
+      gpe_status s_ = (expr);                                                                     \
+      if (s_ != GPE_OK) return s_;                                                                \
+   } while (0)
+
+struct gpe_solver {
+   gpe_params p;
+   int dev = 0;
+   cudaStream_t st = nullptr;
+   bool own_stream = false;
+   bool cplx = false, fp32 = false;
+   Dims d{};
+   double par = 1.;
+   FftPlan px{}, py{}, pz{};
+   int NP = 1, LY = 1, WX = 1;
+   size_t esz_psi = 8, esz_c = 16, esz_r = 8;
+   void *psi = nullptr, *beta = nullptr, *spec = nullptr, *phi = nullptr;
+   void *twx = nullptr, *twy = nullptr, *twz = nullptr;
+   double *udd = nullptr;
+   void *alpha[3] = {nullptr, nullptr, nullptr}, *gamma[3] = {nullptr, nullptr, nullptr};
+   double2 A[3], A0r[3], mA[3];
+   double *x2 = nullptr, *y2 = nullptr, *z2 = nullptr;
+   double *rowA = nullptr, *rowB = nullptr, *tmp = nullptr, *obs = nullptr;
+   State *state = nullptr;
+   std::vector<double> hx, hy, hz, hx2, hy2, hz2;
+   long long launches = 0;
+   size_t obs_cap = 0;
+   // per-kernel profiling: when prof_ev is set, mark() records an event
+   // after every kernel of a step
+   cudaEvent_t *prof_ev = nullptr;
+   int prof_i = 0, prof_cap = 0;
+};
+
+static void mark(gpe_solver *s) {
+   if (s->prof_ev && s->prof_i < s->prof_cap) cudaEventRecord(s->prof_ev[s->prof_i++], s->st);
+}
+
+// ---------------------------------------------------------------- planning
+static bool make_plan(int n, FftPlan &pl) {
+   pl.n = n;
+   pl.nst = 0;
+   int m = n;
+   static const int pref[] = {8, 4, 2, 3, 5};
+   for (int r : pref)
+      while (m % r == 0 && pl.nst < kMaxStages) { pl.rad[pl.nst++] = r; m /= r; }
+   return m == 1;
+}
+
+static int floor_pow2(long long v) {
+   int r = 1;
+   while ((long long) r * 2 <= v) r *= 2;
+   return r;
+}
+
+static gpe_status validate(const gpe_params *p) {
+   if (!p) return fail(GPE_ERR_PARAM, "null parameters");
+   if (p->mode != GPE_MODE_IMAG && p->mode != GPE_MODE_REAL) return fail(GPE_ERR_PARAM, "mode must be 0 (imag) or 1 (real)");
+   if (p->precision != GPE_PREC_FP64 && p->precision != GPE_PREC_MIXED) return fail(GPE_ERR_PARAM, "precision must be 0 or 1");
+   const long n[3] = {p->nx, p->ny, p->nz};
+   for (int a = 0; a < 3; a++) {
+      if (n[a] < 8 || n[a] > 1024) return fail(GPE_ERR_PARAM, "grid sizes must be in [8, 1024]");
+      if (n[a] % 2) return fail(GPE_ERR_PARAM, "grid sizes must be even (k-grid of initpotdd)");
+      FftPlan pl;
+      if (!make_plan((int) n[a], pl)) return fail(GPE_ERR_PARAM, "grid sizes must factor into 2, 3 and 5");
+   }
+   if (!(p->dx > 0 && p->dy > 0 && p->dz > 0 && p->dt > 0)) return fail(GPE_ERR_PARAM, "DX, DY, DZ, DT must be positive");
+   if (!(p->cutoff > 0)) return fail(GPE_ERR_PARAM, "CUTOFF must be positive");
+   return GPE_OK;
+}
+
+static size_t psi_esz(const gpe_params *p) {
+   size_t r = (p->precision == GPE_PREC_MIXED) ? 4 : 8;
+   return p->mode == GPE_MODE_REAL ? 2 * r : r;
+}
+
+extern "C" gpe_status gpe_device_bytes(const gpe_params *p, long long *bytes) {
+   CKS(validate(p));
+   const long long npts = p->nx * p->ny * p->nz;
+   const long long nzh = p->nz / 2 + 1;
+   const size_t r = (p->precision == GPE_PREC_MIXED) ? 4 : 8;
+   long long b = 0;
+   b += 2 * npts * (long long) psi_esz(p);               // psi + beta
+   b += nzh * p->nx * p->ny * (long long) (2 * r);       // spectrum
+   b += npts * (long long) r;                            // phi
+   b += nzh * (p->nx / 2 + 1) * (p->ny / 2 + 1) * 8;     // Udd octant
+   b += 4 * p->nx * p->ny * 8;                           // row sums
+   b += 1 << 20;                                         // tables, state
+   if (bytes) *bytes = b;
+   return GPE_OK;
+}
+
+// ------------------------------------------------------------------ tables
+template <class T> static gpe_status upload(void **dst, const T *src, size_t n) {
+   CK(cudaMalloc(dst, sizeof(T) * n));
+   CK(cudaMemcpy(*dst, src, sizeof(T) * n, cudaMemcpyHostToDevice));
+   return GPE_OK;
+}
+
+static gpe_status make_twiddles(gpe_solver *s, int n, void **dst) {
+   std::vector<double2> t(n);
+   for (int m = 0; m < n; m++) {
+      const long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double) m / (long double) n;
+      t[m] = make_double2((double) cosl(a), (double) sinl(a));
+   }
+   if (s->fp32) {
+      std::vector<float2> f(n);
+      for (int m = 0; m < n; m++) f[m] = make_float2((float) t[m].x, (float) t[m].y);
+      return upload(dst, f.data(), n);
+   }
+   return upload(dst, t.data(), n);
+}
+
+// gencoef (imag3d-mpicuda.cu:894-931, real3d-mpicuda.cu:991-1035).
+static gpe_status make_coef(gpe_solver *s, int ax, long n, double d2) {
+   const double c = s->p.dt / d2 / (3. - s->par);
+   typedef std::complex<double> Z;
+   Z A0, A0r, A, mA;
+   if (!s->cplx) {
+      A0 = 1. + c; A0r = 1. - c; A = -0.5 * c; mA = -A;
+   } else {
+      A0 = Z(1., c); A0r = std::conj(A0); A = Z(0., -0.5 * c); mA = Z(0., -A.imag());
+   }
+   std::vector<Z> al(n - 1), ga(n - 1);
+   al[n - 2] = 0.;
+   ga[n - 2] = Z(-1.) / A0;
+   for (long i = n - 2; i > 0; i--) {
+      al[i - 1] = A * ga[i];
+      ga[i - 1] = Z(-1.) / (A0 + A * al[i - 1]);
+   }
+   s->A[ax] = make_double2(A.real(), A.imag());
+   s->A0r[ax] = make_double2(A0r.real(), A0r.imag());
+   s->mA[ax] = make_double2(mA.real(), mA.imag());
+   if (!s->cplx) {
+      std::vector<double> a(n - 1), g(n - 1);
+      for (long i = 0; i < n - 1; i++) { a[i] = al[i].real(); g[i] = ga[i].real(); }
+      CKS(upload(&s->alpha[ax], a.data(), n - 1));
+      CKS(upload(&s->gamma[ax], g.data(), n - 1));
+   } else {
+      std::vector<double2> a(n - 1), g(n - 1);
+      for (long i = 0; i < n - 1; i++) {
+         a[i] = make_double2(al[i].real(), al[i].imag());
+         g[i] = make_double2(ga[i].real(), ga[i].imag());
+      }
+      CKS(upload(&s->alpha[ax], a.data(), n - 1));
+      CKS(upload(&s->gamma[ax], g.data(), n - 1));
+   }
+   return GPE_OK;
+}
+
+// initpotdd (imag3d-mpicuda.cu:945-980) on the octant |kx| <= nx/2,
+// |ky| <= ny/2, kz <= nz/2: Udd depends on kx^2, ky^2, kz^2 only, and the
+// squares of the reference's negative k values equal those of the octant.
+static gpe_status make_udd(gpe_solver *s) {
+   const long nx = s->p.nx, ny = s->p.ny, nz = s->p.nz;
+   const long nxh = nx / 2 + 1, nyh = ny / 2 + 1, nzh = nz / 2 + 1;
+   const double pi = kRefPi, cutoff = s->p.cutoff;
+   const double dkx = 2. * pi / (nx * s->p.dx), dky = 2. * pi / (ny * s->p.dy), dkz = 2. * pi / (nz * s->p.dz);
+   std::vector<double> kx2(nxh), ky2(nyh), kz2(nzh);
+   for (long i = 0; i < nxh; i++) { double k = i * dkx; kx2[i] = k * k; }
+   for (long i = 0; i < nyh; i++) { double k = i * dky; ky2[i] = k * k; }
+   for (long i = 0; i < nzh; i++) { double k = i * dkz; kz2[i] = k * k; }
+   std::vector<double> u((size_t) (nzh * nxh * nyh));
+   for (long k = 0; k < nzh; k++)
+      for (long i = 0; i < nxh; i++)
+         for (long j = 0; j < nyh; j++) {
+            const double xk = std::sqrt(kz2[k] + kx2[i] + ky2[j]);
+            const double tmp = 1. + 3. * std::cos(xk * cutoff) / (xk * xk * cutoff * cutoff) -
+                               3. * std::sin(xk * cutoff) / (xk * xk * xk * cutoff * cutoff * cutoff);
+            u[(size_t) ((k * nxh + i) * nyh + j)] = (4. * pi * (3. * kz2[k] / (kx2[i] + ky2[j] + kz2[k]) - 1.) / 3.) * tmp;
+         }
+   u[0] = 0.;  // imag3d-mpicuda.cu:975-977
+   void *dp = nullptr;
+   CKS(upload(&dp, u.data(), u.size()));
+   s->udd = (double *) dp;
+   return GPE_OK;
+}
+
+static void free_all(gpe_solver *s) {
+   void *ptrs[] = {s->psi, s->beta, s->spec, s->phi, s->twx, s->twy, s->twz, s->udd, s->x2, s->y2, s->z2,
+                   s->rowA, s->rowB, s->tmp, s->obs, s->state};
+   for (void *q : ptrs)
+      if (q) cudaFree(q);
+   for (int a = 0; a < 3; a++) {
+      if (s->alpha[a]) cudaFree(s->alpha[a]);
+      if (s->gamma[a]) cudaFree(s->gamma[a]);
+   }
+   if (s->own_stream && s->st) cudaStreamDestroy(s->st);
+}
+
+static gpe_status create_impl(const gpe_params *p, void *stream, gpe_solver *s) {
+   s->p = *p;
+   s->cplx = p->mode == GPE_MODE_REAL;
+   s->fp32 = p->precision == GPE_PREC_MIXED;
+   s->par = (p->opt == 2) ? 2. : 1.;
+   if (p->device >= 0) CK(cudaSetDevice(p->device));
+   CK(cudaGetDevice(&s->dev));
+   if (stream) {
+      s->st = (cudaStream_t) stream;
+   } else {
+      CK(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+      s->own_stream = true;
+   }
+   Dims &d = s->d;
+   d.nx = (int) p->nx; d.ny = (int) p->ny; d.nz = (int) p->nz; d.nzh = d.nz / 2 + 1;
+   d.nxy = (long long) d.nx * d.ny;
+   d.npts = d.nxy * d.nz;
+   make_plan(d.nx, s->px);
+   make_plan(d.ny, s->py);
+   make_plan(d.nz, s->pz);
+   const size_t r = s->fp32 ? 4 : 8;
+   s->esz_r = r;
+   s->esz_c = 2 * r;
+   s->esz_psi = psi_esz(p);
+   // tile sizes: ~64 KB of ping-pong shared memory per CTA
+   const long long budget = 64 * 1024;
+   s->NP = std::min(32, floor_pow2(std::max(1LL, budget / (long long) (2 * (d.nz + 2) * s->esz_c))));
+   s->LY = std::min(32, floor_pow2(std::max(1LL, budget / (long long) (2 * d.ny * s->esz_c))));
+   s->WX = std::max(4, std::min(16, floor_pow2(std::max(1LL, budget / (long long) (2 * d.nx * s->esz_c)))));
+
+   CK(cudaMalloc(&s->psi, s->esz_psi * d.npts));
+   CK(cudaMalloc(&s->beta, s->esz_psi * d.npts));
+   CK(cudaMalloc(&s->spec, s->esz_c * (size_t) d.nzh * d.nxy));
+   CK(cudaMalloc(&s->phi, r * d.npts));
+   CK(cudaMemset(s->psi, 0, s->esz_psi * d.npts));
+   CK(cudaMalloc(&s->rowA, sizeof(double) * d.nxy));
+   CK(cudaMalloc(&s->rowB, sizeof(double) * d.nxy));
+   CK(cudaMalloc(&s->tmp, sizeof(double) * std::max<long long>(d.nxy, std::max(d.nx, std::max(d.ny, d.nz))) * 2));
+   s->obs_cap = 64;
+   CK(cudaMalloc(&s->obs, sizeof(double) * s->obs_cap));
+   CK(cudaMalloc(&s->state, sizeof(State)));
+   State st0{};
+   st0.norm = 1.; st0.scale = 1.; st0.scale2 = 1.;
+   CK(cudaMemcpy(s->state, &st0, sizeof(State), cudaMemcpyHostToDevice));
+
+   CKS(make_twiddles(s, d.nx, &s->twx));
+   CKS(make_twiddles(s, d.ny, &s->twy));
+   CKS(make_twiddles(s, d.nz, &s->twz));
+   CKS(make_coef(s, 0, d.nx, p->dx * p->dx));
+   CKS(make_coef(s, 1, d.ny, p->dy * p->dy));
+   CKS(make_coef(s, 2, d.nz, p->dz * p->dz));
+   CKS(make_udd(s));
+
+   // space mesh (initpsi, imag3d-mpicuda.cu:842-855)
+   const long nx2 = d.nx / 2, ny2 = d.ny / 2, nz2 = d.nz / 2;
+   s->hx.resize(d.nx); s->hy.resize(d.ny); s->hz.resize(d.nz);
+   s->hx2.resize(d.nx); s->hy2.resize(d.ny); s->hz2.resize(d.nz);
+   for (long i = 0; i < d.nx; i++) { s->hx[i] = (i - nx2) * p->dx; s->hx2[i] = s->hx[i] * s->hx[i]; }
+   for (long j = 0; j < d.ny; j++) { s->hy[j] = (j - ny2) * p->dy; s->hy2[j] = s->hy[j] * s->hy[j]; }
+   for (long k = 0; k < d.nz; k++) { s->hz[k] = (k - nz2) * p->dz; s->hz2[k] = s->hz[k] * s->hz[k]; }
+   void *t = nullptr;
+   CKS(upload(&t, s->hx2.data(), d.nx)); s->x2 = (double *) t;
+   CKS(upload(&t, s->hy2.data(), d.ny)); s->y2 = (double *) t;
+   CKS(upload(&t, s->hz2.data(), d.nz)); s->z2 = (double *) t;
+   CK(cudaDeviceSynchronize());
+   return GPE_OK;
+}
+
+extern "C" gpe_status gpe_create(const gpe_params *p, void *stream, gpe_solver **out) {
+   if (!out) return fail(GPE_ERR_PARAM, "null output handle");
+   *out = nullptr;
+   CKS(validate(p));
+   gpe_solver *s = new gpe_solver();
+   gpe_status st = create_impl(p, stream, s);
+   if (st != GPE_OK) {
+      std::string keep = g_err;
+      free_all(s);
+      delete s;
+      g_err = keep;
+      return st;
+   }
+   *out = s;
+   return GPE_OK;
+}
+
+extern "C" void gpe_destroy(gpe_solver *s) {
+   if (!s) return;
+   if (s->st) cudaStreamSynchronize(s->st);
+   free_all(s);
+   delete s;
+}
+
+extern "C" const char *gpe_last_error(void) { return g_err.c_str(); }
+
+// ------------------------------------------------------------------ launches
+static Trap trap_of(const gpe_solver *s) {
+   Trap t;
+   t.x2 = s->x2; t.y2 = s->y2; t.z2 = s->z2;
+   t.hp = 0.5 * s->par;
+   t.vg2 = s->p.gamma * s->p.gamma;
+   t.vn2 = s->p.nu * s->p.nu;
+   t.vl2 = s->p.lambda * s->p.lambda;
+   return t;
+}
+
+static Coef coef_of(const gpe_solver *s, int ax) {
+   Coef c;
+   c.alpha = s->alpha[ax];
+   c.gamma = s->gamma[ax];
+   c.A = s->A[ax];
+   c.A0r = s->A0r[ax];
+   c.mA = s->mA[ax];
+   return c;
+}
+
+static unsigned blocks_for(long long n, int bs) { return (unsigned) ((n + bs - 1) / bs); }
+
+template <class R, bool CPLX> struct Impl {
+   using P = typename Tr<R, CPLX>::P;
+   using C = cpx<R>;
+
+   static gpe_status smem_attr(const void *f, size_t bytes) {
+      if (bytes > 48 * 1024) CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bytes));
+      return GPE_OK;
+   }
+
+   static gpe_status psidd2(gpe_solver *s) {
+      const Dims &d = s->d;
+      C *spec = (C *) s->spec;
+      {
+         const size_t sm = (size_t) (2 * s->NP * (d.nz + 2) + d.nz) * sizeof(C);
+         CKS(smem_attr((const void *) k_zfwd<R, CPLX>, sm));
+         k_zfwd<R, CPLX><<<blocks_for(d.nxy, 2 * s->NP), 256, sm, s->st>>>((const P *) s->psi, spec, d, s->pz,
+                                                                            (const C *) s->twz, s->NP);
+         CKL();
+         mark(s);
+      }
+      const size_t smy = (size_t) (2 * s->LY * d.ny + d.ny) * sizeof(C);
+      const unsigned gy = blocks_for((long long) d.nzh * d.nx, s->LY);
+      CKS(smem_attr((const void *) k_yfft<R, false>, smy));
+      k_yfft<R, false><<<gy, 256, smy, s->st>>>(spec, d, s->py, (const C *) s->twy, s->LY);
+      CKL();
+      mark(s);
+      {
+         const size_t sm = (size_t) (2 * d.nx * s->WX + d.nx) * sizeof(C);
+         const unsigned gx = (unsigned) (d.nzh * ((d.ny + s->WX - 1) / s->WX));
+         CKS(smem_attr((const void *) k_xconv<R>, sm));
+         k_xconv<R><<<gx, 256, sm, s->st>>>(spec, d, s->px, (const C *) s->twx, s->udd, s->state, s->WX);
+         CKL();
+         mark(s);
+      }
+      CKS(smem_attr((const void *) k_yfft<R, true>, smy));
+      k_yfft<R, true><<<gy, 256, smy, s->st>>>(spec, d, s->py, (const C *) s->twy, s->LY);
+      CKL();
+      mark(s);
+      {
+         const size_t sm = (size_t) (2 * s->NP * (d.nz + 2) + d.nz) * sizeof(C);
+         CKS(smem_attr((const void *) k_zinv<R>, sm));
+         k_zinv<R><<<blocks_for(d.nxy, 2 * s->NP), 256, sm, s->st>>>(spec, (R *) s->phi, d, s->pz, (const C *) s->twz,
+                                                                      s->NP);
+         CKL();
+         mark(s);
+      }
+      k_phifix<R><<<256, 256, 0, s->st>>>((R *) s->phi, d);
+      CKL();
+      mark(s);
+      s->launches += 6;
+      return GPE_OK;
+   }
+
+   static gpe_status xsweep(gpe_solver *s, bool nu, double g, double gd) {
+      const Dims &d = s->d;
+      const long long nl = (long long) d.ny * d.nz;
+      if (nu)
+         k_xsweep<R, CPLX, true><<<blocks_for(nl, 128), 128, 0, s->st>>>((P *) s->psi, (P *) s->beta, (const R *) s->phi,
+                                                                          d, coef_of(s, 0), trap_of(s), g, gd, s->p.dt,
+                                                                          s->state);
+      else
+         k_xsweep<R, CPLX, false><<<blocks_for(nl, 128), 128, 0, s->st>>>((P *) s->psi, (P *) s->beta,
+                                                                           (const R *) s->phi, d, coef_of(s, 0),
+                                                                           trap_of(s), g, gd, s->p.dt, s->state);
+      CKL();
+      mark(s);
+      s->launches++;
+      return GPE_OK;
+   }
+
+   static gpe_status ysweep(gpe_solver *s) {
+      const Dims &d = s->d;
+      k_ysweep<R, CPLX><<<blocks_for((long long) d.nx * d.nz, 128), 128, 0, s->st>>>((P *) s->psi, (P *) s->beta, d,
+                                                                                   coef_of(s, 1));
+      CKL();
+      mark(s);
+      s->launches++;
+      return GPE_OK;
+   }
+
+   static gpe_status zsweep(gpe_solver *s, bool simp) {
+      const Dims &d = s->d;
+      if (simp)
+         k_zsweep<R, CPLX, true><<<blocks_for(d.nxy, 128), 128, 0, s->st>>>((P *) s->psi, (P *) s->beta, d,
+                                                                             coef_of(s, 2), s->rowA, s->p.dz);
+      else
+         k_zsweep<R, CPLX, false><<<blocks_for(d.nxy, 128), 128, 0, s->st>>>((P *) s->psi, (P *) s->beta, d,
+                                                                              coef_of(s, 2), s->rowA, s->p.dz);
+      CKL();
+      mark(s);
+      s->launches++;
+      return GPE_OK;
+   }
+
+   static gpe_status norm_final(gpe_solver *s, double *dev_out) {
+      k_norm_final<<<1, 256, sizeof(double) * s->d.nx, s->st>>>(s->rowA, s->d, s->p.dx, s->p.dy, s->state, dev_out);
+      CKL();
+      mark(s);
+      s->launches++;
+      return GPE_OK;
+   }
+
+   static gpe_status apply_scale(gpe_solver *s) {
+      k_apply_scale<R, CPLX><<<592, 256, 0, s->st>>>((P *) s->psi, s->d.npts, s->state);
+      CKL();
+      k_state_set<<<1, 1, 0, s->st>>>(s->state, 1.);
+      CKL();
+      s->launches += 2;
+      return GPE_OK;
+   }
+
+   static gpe_status calcnorm(gpe_solver *s, bool renorm) {
+      const Dims &d = s->d;
+      k_rows_dens<R, CPLX><<<blocks_for(d.nxy, 128), 128, 0, s->st>>>((const P *) s->psi, d, s->p.dz, s->rowA, nullptr,
+                                                                     s->z2);
+      CKL();
+      CKS(norm_final(s, s->obs));
+      s->launches++;
+      if (renorm) {
+         CKS(apply_scale(s));
+      } else {
+         k_state_set<<<1, 1, 0, s->st>>>(s->state, 1.);
+         CKL();
+      }
+      return GPE_OK;
+   }
+
+   static gpe_status rms(gpe_solver *s, double *dev_out) {
+      const Dims &d = s->d;
+      k_rows_dens<R, CPLX><<<blocks_for(d.nxy, 128), 128, 0, s->st>>>((const P *) s->psi, d, s->p.dz, s->rowA, s->rowB,
+                                                                     s->z2);
+      CKL();
+      k_rms_final<<<1, 256, sizeof(double) * 3 * d.nx, s->st>>>(s->rowA, s->rowB, d, s->p.dx, s->p.dy, s->x2, s->y2,
+                                                                 dev_out);
+      CKL();
+      s->launches += 2;
+      return GPE_OK;
+   }
+
+   static gpe_status muen(gpe_solver *s, double g, double gd, double *dev_out) {
+      const Dims &d = s->d;
+      CKS(psidd2(s));
+      k_muen_rows<R, CPLX><<<blocks_for(d.nxy, 128), 128, 0, s->st>>>((const P *) s->psi, (const R *) s->phi, d,
+                                                                     trap_of(s), g, gd, s->p.dx, s->p.dy, s->p.dz,
+                                                                     s->par, s->rowA, s->rowB);
+      CKL();
+      k_xy_final<<<1, 256, sizeof(double) * d.nx, s->st>>>(s->rowA, d, s->p.dx, s->p.dy, dev_out);
+      CKL();
+      k_xy_final<<<1, 256, sizeof(double) * d.nx, s->st>>>(s->rowB, d, s->p.dx, s->p.dy, dev_out + 1);
+      CKL();
+      s->launches += 3;
+      return GPE_OK;
+   }
+
+   // One split step (imag3d-mpicuda.cu:319-324): calcpsidd2, calcnu (fused
+   // into the x sweep), x, y, z sweeps, and in imaginary time the norm.
+   static gpe_status step(gpe_solver *s, double g, double gd, double *dev_norm) {
+      CKS(psidd2(s));
+      CKS(xsweep(s, true, g, gd));
+      CKS(ysweep(s));
+      const bool imag = !CPLX;
+      CKS(zsweep(s, imag));
+      if (imag) CKS(norm_final(s, dev_norm));
+      return GPE_OK;
+   }
+
+   static gpe_status calcnu(gpe_solver *s, double g, double gd) {
+      k_calcnu<R, CPLX><<<592, 256, 0, s->st>>>((P *) s->psi, (const R *) s->phi, s->d, trap_of(s), g, gd, s->p.dt);
+      CKL();
+      s->launches++;
+      return GPE_OK;
+   }
+
+   static gpe_status density(gpe_solver *s, int kind, long sx, long sy, long sz, double *out, long cap, long *count);
+};
+
+template <class R, bool CPLX>
+gpe_status Impl<R, CPLX>::density(gpe_solver *s, int kind, long sx, long sy, long sz, double *out, long cap,
+                                  long *count) {
+   const Dims &d = s->d;
+   const P *psi = (const P *) s->psi;
+   const double hh[3] = {s->p.dx, s->p.dy, s->p.dz};
+   const int n[3] = {d.nx, d.ny, d.nz};
+   const std::vector<double> *crd[3] = {&s->hx, &s->hy, &s->hz};
+   const long stp[3] = {sx, sy, sz};
+   std::vector<double> buf;
+   long o = 0;
+   auto need = [&](long m) -> gpe_status {
+      if (m > cap) return fail(GPE_ERR_PARAM, "density output buffer too small");
+      return GPE_OK;
+   };
+   if (kind >= GPE_DEN_1D_X && kind <= GPE_DEN_1D_Z) {
+      // axis integrated first, then the second one (reference nesting)
+      const int keep = kind - GPE_DEN_1D_X;
+      const int first = (keep == 2) ? 1 : 2;   // z (or y for the z profile)
+      const int second = (keep == 0) ? 1 : 0;  // y for x profile, x otherwise
+      const int o1 = first == 0 ? 1 : 0, o2 = first == 2 ? 1 : 2;  // axes of the 2D result
+      k_lineint_psi<R, CPLX><<<blocks_for((long long) n[o1] * n[o2], 128), 128, 0, s->st>>>(psi, d, first, hh[first],
+                                                                                          s->rowA);
+      CKL();
+      const int ax = (second == o1) ? 0 : 1;  // integrate rows (0) or columns (1)
+      const int m = n[keep];
+      k_lineint_arr<<<blocks_for(m, 128), 128, 0, s->st>>>(s->rowA, n[o1], n[o2], ax == 0 ? 0 : 1, hh[second], s->tmp);
+      CKL();
+      s->launches += 2;
+      buf.resize(m);
+      CK(cudaMemcpyAsync(buf.data(), s->tmp, sizeof(double) * m, cudaMemcpyDeviceToHost, s->st));
+      CK(cudaStreamSynchronize(s->st));
+      for (long c = 0; c < m; c += stp[keep]) {
+         CKS(need(o + 2));
+         out[o++] = (*crd[keep])[c];
+         out[o++] = buf[c];
+      }
+   } else if (kind >= GPE_DEN_2D_XY && kind <= GPE_DEN_2D_YZ) {
+      const int integ = 2 - (kind - GPE_DEN_2D_XY);  // xy -> z, xz -> y, yz -> x
+      const int a1 = integ == 0 ? 1 : 0, a2 = integ == 2 ? 1 : 2;
+      k_lineint_psi<R, CPLX><<<blocks_for((long long) n[a1] * n[a2], 128), 128, 0, s->st>>>(psi, d, integ, hh[integ],
+                                                                                          s->rowA);
+      CKL();
+      s->launches++;
+      buf.resize((size_t) n[a1] * n[a2]);
+      CK(cudaMemcpyAsync(buf.data(), s->rowA, sizeof(double) * buf.size(), cudaMemcpyDeviceToHost, s->st));
+      CK(cudaStreamSynchronize(s->st));
+      for (long u = 0; u < n[a1]; u += stp[a1])
+         for (long v = 0; v < n[a2]; v += stp[a2]) {
+            CKS(need(o + 3));
+            out[o++] = (*crd[a1])[u];
+            out[o++] = (*crd[a2])[v];
+            out[o++] = buf[(size_t) u * n[a2] + v];
+         }
+   } else if (kind >= GPE_DEN_3D_XY0 && kind <= GPE_DEN_3D_0YZ) {
+      const int fixed = 2 - (kind - GPE_DEN_3D_XY0);  // xy0 -> z fixed, x0z -> y, 0yz -> x
+      const int a1 = fixed == 0 ? 1 : 0, a2 = fixed == 2 ? 1 : 2;
+      int lo[3] = {0, 0, 0}, hi[3] = {d.nx, d.ny, d.nz}, sp[3] = {(int) sx, (int) sy, (int) sz};
+      lo[fixed] = n[fixed] / 2; hi[fixed] = lo[fixed] + 1; sp[fixed] = 1;
+      const long na = (n[a1] + stp[a1] - 1) / stp[a1], nb = (n[a2] + stp[a2] - 1) / stp[a2];
+      double *dv = nullptr;
+      CK(cudaMalloc(&dv, sizeof(double) * na * nb));
+      k_gather_dens<R, CPLX><<<blocks_for(na * nb, 256), 256, 0, s->st>>>(psi, d, lo[0], hi[0], sp[0], lo[1], hi[1], sp[1],
+                                                                         lo[2], hi[2], sp[2], dv);
+      s->launches++;
+      buf.resize(na * nb);
+      cudaError_t e1 = cudaGetLastError();
+      cudaError_t e2 = cudaMemcpyAsync(buf.data(), dv, sizeof(double) * buf.size(), cudaMemcpyDeviceToHost, s->st);
+      cudaError_t e3 = cudaStreamSynchronize(s->st);
+      cudaFree(dv);
+      if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) return fail(GPE_ERR_CUDA, "density cut failed");
+      for (long u = 0; u < na; u++)
+         for (long v = 0; v < nb; v++) {
+            CKS(need(o + 3));
+            out[o++] = (*crd[a1])[u * stp[a1]];
+            out[o++] = (*crd[a2])[v * stp[a2]];
+            out[o++] = buf[(size_t) u * nb + v];
+         }
+   } else if (kind == GPE_DEN_3D) {
+      const long na = (d.nx + sx - 1) / sx, nb = (d.ny + sy - 1) / sy, nc = (d.nz + sz - 1) / sz;
+      CKS(need(na * nb * nc));
+      double *dv = nullptr;
+      CK(cudaMalloc(&dv, sizeof(double) * na * nb * nc));
+      k_gather_dens<R, CPLX><<<592, 256, 0, s->st>>>(psi, d, 0, d.nx, (int) sx, 0, d.ny, (int) sy, 0, d.nz, (int) sz, dv);
+      s->launches++;
+      cudaError_t e1 = cudaGetLastError();
+      cudaError_t e2 = cudaMemcpyAsync(out, dv, sizeof(double) * na * nb * nc, cudaMemcpyDeviceToHost, s->st);
+      cudaError_t e3 = cudaStreamSynchronize(s->st);
+      cudaFree(dv);
+      if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) return fail(GPE_ERR_CUDA, "density copy failed");
+      o = na * nb * nc;
+   } else {
+      return fail(GPE_ERR_PARAM, "unknown density kind");
+   }
+   if (count) *count = o;
+   return GPE_OK;
+}
+
+#define DISPATCH(s, CALL)                                                                 \
+   (((s)->fp32) ? (((s)->cplx) ? Impl<float, true>::CALL : Impl<float, false>::CALL)     \
+                : (((s)->cplx) ? Impl<double, true>::CALL : Impl<double, false>::CALL))
+
+#define CHECK_HANDLE(s) \
+   if (!(s)) return fail(GPE_ERR_PARAM, "null solver handle")
+
+// ------------------------------------------------------------------ psi I/O
+// FP64 psi is copied as is (the host layout equals the device layout); the
+// mixed-precision handle converts through a host float buffer.
+extern "C" gpe_status gpe_set_psi(gpe_solver *s, const double *psi) {
+   CHECK_HANDLE(s);
+   if (!psi) return fail(GPE_ERR_PARAM, "null psi");
+   CK(cudaSetDevice(s->dev));
+   const size_t nd = (size_t) s->d.npts * (s->cplx ? 2 : 1);
+   if (s->fp32) {
+      std::vector<float> b(nd);
+      for (size_t q = 0; q < nd; q++) b[q] = (float) psi[q];
+      CK(cudaMemcpyAsync(s->psi, b.data(), sizeof(float) * nd, cudaMemcpyHostToDevice, s->st));
+      CK(cudaStreamSynchronize(s->st));
+   } else {
+      CK(cudaMemcpyAsync(s->psi, psi, sizeof(double) * nd, cudaMemcpyHostToDevice, s->st));
+      CK(cudaStreamSynchronize(s->st));
+   }
+   k_state_set<<<1, 1, 0, s->st>>>(s->state, 1.);
+   CKL();
+   return GPE_OK;
+}
+
+extern "C" gpe_status gpe_get_psi(gpe_solver *s, double *psi) {
+   CHECK_HANDLE(s);
+   if (!psi) return fail(GPE_ERR_PARAM, "null psi");
+   CK(cudaSetDevice(s->dev));
+   const size_t nd = (size_t) s->d.npts * (s->cplx ? 2 : 1);
+   if (s->fp32) {
+      std::vector<float> b(nd);
+      CK(cudaMemcpyAsync(b.data(), s->psi, sizeof(float) * nd, cudaMemcpyDeviceToHost, s->st));
+      CK(cudaStreamSynchronize(s->st));
+      for (size_t q = 0; q < nd; q++) psi[q] = b[q];
+   } else {
+      CK(cudaMemcpyAsync(psi, s->psi, sizeof(double) * nd, cudaMemcpyDeviceToHost, s->st));
+      CK(cudaStreamSynchronize(s->st));
+   }
+   return GPE_OK;
+}
+
+// initpsi Gaussian (imag3d-mpicuda.cu:835-867), evaluated on the host like
+// the reference and uploaded.
+extern "C" gpe_status gpe_init_gaussian(gpe_solver *s) {
+   CHECK_HANDLE(s);
+   const double pi = kRefPi;
+   const double cpsi = std::sqrt(pi * std::sqrt(pi / (s->p.gamma * s->p.nu * s->p.lambda)));
+   const Dims &d = s->d;
+   std::vector<double> re((size_t) d.npts * (s->cplx ? 2 : 1), 0.);
+   for (long i = 0; i < d.nx; i++)
+      for (long j = 0; j < d.ny; j++)
+         for (long k = 0; k < d.nz; k++) {
+            const double tmp = std::exp(-0.5 * (s->p.gamma * s->hx2[i] + s->p.nu * s->hy2[j] + s->p.lambda * s->hz2[k]));
+            re[(size_t) ((i * d.ny + j) * d.nz + k) * (s->cplx ? 2 : 1)] = tmp / cpsi;
+         }
+   return gpe_set_psi(s, re.data());
+}
+
+extern "C" gpe_status gpe_init_density(gpe_solver *s, const double *rho) {
+   CHECK_HANDLE(s);
+   if (!rho) return fail(GPE_ERR_PARAM, "null density");
+   CK(cudaSetDevice(s->dev));
+   double *dr = nullptr;
+   CK(cudaMalloc(&dr, sizeof(double) * s->d.npts));
+   cudaError_t e = cudaMemcpyAsync(dr, rho, sizeof(double) * s->d.npts, cudaMemcpyHostToDevice, s->st);
+   if (e == cudaSuccess) {
+      if (s->fp32)
+         s->cplx ? k_init_density<float, true><<<592, 256, 0, s->st>>>((float2 *) s->psi, dr, s->d.npts)
+                 : k_init_density<float, false><<<592, 256, 0, s->st>>>((float *) s->psi, dr, s->d.npts);
+      else
+         s->cplx ? k_init_density<double, true><<<592, 256, 0, s->st>>>((double2 *) s->psi, dr, s->d.npts)
+                 : k_init_density<double, false><<<592, 256, 0, s->st>>>((double *) s->psi, dr, s->d.npts);
+      e = cudaGetLastError();
+   }
+   cudaError_t e2 = cudaStreamSynchronize(s->st);
+   cudaFree(dr);
+   if (e != cudaSuccess || e2 != cudaSuccess) return fail(GPE_ERR_CUDA, "init from density failed");
+   s->launches++;
+   k_state_set<<<1, 1, 0, s->st>>>(s->state, 1.);
+   CKL();
+   return GPE_OK;
+}
+
+// -------------------------------------------------------------- operators
+static gpe_status read_obs(gpe_solver *s, double *dst, int n, int off = 0) {
+   CK(cudaMemcpyAsync(dst, s->obs + off, sizeof(double) * n, cudaMemcpyDeviceToHost, s->st));
+   CK(cudaStreamSynchronize(s->st));
+   return GPE_OK;
+}
+
+extern "C" gpe_status gpe_calcnorm(gpe_solver *s, int renormalize, double *norm) {
+   CHECK_HANDLE(s);
+   CK(cudaSetDevice(s->dev));
+   CKS(DISPATCH(s, calcnorm(s, renormalize != 0)));
+   double v = 0;
+   CKS(read_obs(s, &v, 1));
+   if (norm) *norm = v;
+   return GPE_OK;
+}
+
+extern "C" gpe_status gpe_run(gpe_solver *s, long nsteps, double *g, double *gd, double g_inc, double gd_inc,
+                              double *last_norm, long rms_every, double *rms_out) {
+   CHECK_HANDLE(s);
+   if (!g || !gd) return fail(GPE_ERR_PARAM, "null coupling pointers");
+   if (nsteps < 0) return fail(GPE_ERR_PARAM, "negative step count");
+   CK(cudaSetDevice(s->dev));
+   const bool imag = !s->cplx;
+   long nrms = (rms_every > 0) ? (nsteps + rms_every - 1) / rms_every : 0;
+   double *drms = nullptr;
+   if (nrms > 0) {
+      if (!rms_out) return fail(GPE_ERR_PARAM, "rms_out required when rms_every > 0");
+      CK(cudaMalloc(&drms, sizeof(double) * 4 * nrms));
+   }
+   gpe_status st = GPE_OK;
+   for (long c = 0; c < nsteps && st == GPE_OK; c++) {
+      *g += g_inc;
+      *gd += gd_inc;
+      st = DISPATCH(s, step(s, *g, *gd, s->obs));
+      if (st == GPE_OK && rms_every > 0 && c % rms_every == 0) {
+         if (imag) st = DISPATCH(s, apply_scale(s));
+         if (st == GPE_OK) st = DISPATCH(s, rms(s, drms + 4 * (c / rms_every)));
+      }
+   }
+   if (st == GPE_OK && imag && nsteps > 0) st = DISPATCH(s, apply_scale(s));
+   if (st == GPE_OK && last_norm && imag && nsteps > 0) st = read_obs(s, last_norm, 1);
+   if (drms) {
+      if (st == GPE_OK) {
+         cudaError_t e = cudaMemcpyAsync(rms_out, drms, sizeof(double) * 4 * nrms, cudaMemcpyDeviceToHost, s->st);
+         if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+         if (e != cudaSuccess) st = fail(GPE_ERR_CUDA, cudaGetErrorString(e));
+      }
+      cudaFree(drms);
+   }
+   if (st == GPE_OK) {
+      cudaError_t e = cudaStreamSynchronize(s->st);
+      if (e != cudaSuccess) st = fail(GPE_ERR_CUDA, cudaGetErrorString(e));
+   }
+   return st;
+}
+
+extern "C" gpe_status gpe_calcmuen(gpe_solver *s, double g, double gd, double *mu, double *en) {
+   CHECK_HANDLE(s);
+   CK(cudaSetDevice(s->dev));
+   CKS(DISPATCH(s, muen(s, g, gd, s->obs + 8)));
+   double v[2];
+   CKS(read_obs(s, v, 2, 8));
+   if (mu) *mu = v[0];
+   if (en) *en = v[1];
+   return GPE_OK;
+}
+
+extern "C" gpe_status gpe_calcrms(gpe_solver *s, double *rms) {
+   CHECK_HANDLE(s);
+   if (!rms) return fail(GPE_ERR_PARAM, "null rms");
+   CK(cudaSetDevice(s->dev));
+   CKS(DISPATCH(s, rms(s, s->obs + 16)));
+   return read_obs(s, rms, 4, 16);
+}
+
+extern "C" gpe_status gpe_psi_center2(gpe_solver *s, double *value) {
+   CHECK_HANDLE(s);
+   CK(cudaSetDevice(s->dev));
+   const Dims &d = s->d;
+   const long long q = ((long long) (d.nx / 2) * d.ny + d.ny / 2) * d.nz + d.nz / 2;
+   double v[2] = {0, 0};
+   if (s->fp32) {
+      float f[2] = {0, 0};
+      CK(cudaMemcpyAsync(f, (char *) s->psi + q * s->esz_psi, s->esz_psi, cudaMemcpyDeviceToHost, s->st));
+      CK(cudaStreamSynchronize(s->st));
+      v[0] = f[0]; v[1] = s->cplx ? f[1] : 0.;
+   } else {
+      CK(cudaMemcpyAsync(v, (char *) s->psi + q * s->esz_psi, s->esz_psi, cudaMemcpyDeviceToHost, s->st));
+      CK(cudaStreamSynchronize(s->st));
+      if (!s->cplx) v[1] = 0.;
+   }
+   if (value) *value = v[0] * v[0] + v[1] * v[1];
+   return GPE_OK;
+}
+
+extern "C" gpe_status gpe_density(gpe_solver *s, int kind, long sx, long sy, long sz, double *out, long cap,
+                                  long *count) {
+   CHECK_HANDLE(s);
+   if (!out) return fail(GPE_ERR_PARAM, "null output");
+   if (sx < 1 || sy < 1 || sz < 1) return fail(GPE_ERR_PARAM, "OUTSTPX/Y/Z must be >= 1");
+   CK(cudaSetDevice(s->dev));
+   return DISPATCH(s, density(s, kind, sx, sy, sz, out, cap, count));
+}
+
+extern "C" gpe_status gpe_calcpsidd2(gpe_solver *s) {
+   CHECK_HANDLE(s);
+   CK(cudaSetDevice(s->dev));
+   return DISPATCH(s, psidd2(s));
+}
+
+extern "C" gpe_status gpe_get_phi(gpe_solver *s, double *phi) {
+   CHECK_HANDLE(s);
+   if (!phi) return fail(GPE_ERR_PARAM, "null phi");
+   CK(cudaSetDevice(s->dev));
+   const long long n = s->d.npts;
+   if (s->fp32) {
+      std::vector<float> b((size_t) n);
+      CK(cudaMemcpyAsync(b.data(), s->phi, sizeof(float) * n, cudaMemcpyDeviceToHost, s->st));
+      CK(cudaStreamSynchronize(s->st));
+      for (long long q = 0; q < n; q++) phi[q] = b[(size_t) q];
+   } else {
+      CK(cudaMemcpyAsync(phi, s->phi, sizeof(double) * n, cudaMemcpyDeviceToHost, s->st));
+      CK(cudaStreamSynchronize(s->st));
+   }
+   return GPE_OK;
+}
+
+extern "C" gpe_status gpe_calcnu(gpe_solver *s, double g, double gd) {
+   CHECK_HANDLE(s);
+   CK(cudaSetDevice(s->dev));
+   return DISPATCH(s, calcnu(s, g, gd));
+}
+
+extern "C" gpe_status gpe_calclux(gpe_solver *s) {
+   CHECK_HANDLE(s);
+   CK(cudaSetDevice(s->dev));
+   return DISPATCH(s, xsweep(s, false, 0., 0.));
+}
+
+extern "C" gpe_status gpe_calcluy(gpe_solver *s) {
+   CHECK_HANDLE(s);
+   CK(cudaSetDevice(s->dev));
+   return DISPATCH(s, ysweep(s));
+}
+
+extern "C" gpe_status gpe_calcluz(gpe_solver *s) {
+   CHECK_HANDLE(s);
+   CK(cudaSetDevice(s->dev));
+   return DISPATCH(s, zsweep(s, false));
+}
+
+extern "C" gpe_status gpe_synchronize(gpe_solver *s) {
+   CHECK_HANDLE(s);
+   CK(cudaStreamSynchronize(s->st));
+   return GPE_OK;
+}
+
+extern "C" gpe_status gpe_launch_count(gpe_solver *s, long long *count) {
+   CHECK_HANDLE(s);
+   if (count) *count = s->launches;
+   return GPE_OK;
+}
+
+extern "C" gpe_status gpe_time_steps(gpe_solver *s, long nsteps, double g, double gd, double *ms) {
+   CHECK_HANDLE(s);
+   CK(cudaSetDevice(s->dev));
+   cudaEvent_t a, b;
+   CK(cudaEventCreate(&a));
+   CK(cudaEventCreate(&b));
+   CK(cudaEventRecord(a, s->st));
+   gpe_status st = GPE_OK;
+   for (long c = 0; c < nsteps && st == GPE_OK; c++) st = DISPATCH(s, step(s, g, gd, nullptr));
+   if (st == GPE_OK && !s->cplx) st = DISPATCH(s, apply_scale(s));
+   CK(cudaEventRecord(b, s->st));
+   CK(cudaEventSynchronize(b));
+   float f = 0;
+   CK(cudaEventElapsedTime(&f, a, b));
+   cudaEventDestroy(a);
+   cudaEventDestroy(b);
+   if (ms) *ms = f;
+   return st;
+}
+
+// ------------------------------------------------------------ profiling
+static const char *kStepKernels[] = {"zfwd_r2c", "yfft_fwd", "xconv_udd", "yfft_inv", "zinv_c2r",
+                                     "phi_boundary", "xsweep_calcnu", "ysweep", "zsweep", "norm_final"};
+
+extern "C" const char *gpe_step_kernel_name(gpe_solver *s, int i) {
+   const int n = (s && s->cplx) ? 9 : 10;
+   if (i < 0 || i >= n) return nullptr;
+   if (i == 8 && s && !s->cplx) return "zsweep_norm";
+   return kStepKernels[i];
+}
+
+// Compulsory bytes of one launch of kernel i for this pass structure.
+extern "C" double gpe_step_kernel_bytes(gpe_solver *s, int i) {
+   if (!s) return 0.;
+   const Dims &d = s->d;
+   const double sp = (double) s->esz_psi, sc = (double) s->esz_c, r = (double) s->esz_r;
+   const double npts = (double) d.npts, half = (double) d.nzh * (double) d.nxy;
+   const double oct = (double) d.nzh * (d.nx / 2 + 1) * (d.ny / 2 + 1) * 8.;
+   const double planes = ((double) (d.ny - 1) * (d.nz - 1) + (double) (d.nx - 1) * (d.nz - 1) +
+                          (double) (d.nx - 1) * (d.ny - 1)) * 2. * r;
+   switch (i) {
+   case 0: return npts * sp + half * sc;
+   case 1: case 3: return 2. * half * sc;
+   case 2: return 2. * half * sc + oct;
+   case 4: return half * sc + npts * r;
+   case 5: return planes;
+   case 6: return npts * (2. * sp + r);
+   case 7: return 2. * npts * sp;
+   case 8: return 2. * npts * sp + (s->cplx ? 0. : 8. * (double) d.nxy);
+   case 9: return s->cplx ? 0. : 8. * (double) d.nxy;
+   default: return 0.;
+   }
+}
+
+extern "C" gpe_status gpe_profile_step(gpe_solver *s, long nsteps, double g, double gd, double *ms, int cap,
+                                       int *count) {
+   CHECK_HANDLE(s);
+   if (!ms || nsteps < 1) return fail(GPE_ERR_PARAM, "profile needs an output array and nsteps >= 1");
+   CK(cudaSetDevice(s->dev));
+   const int nk = s->cplx ? 9 : 10;
+   if (cap < nk) return fail(GPE_ERR_PARAM, "profile output array too small");
+   std::vector<cudaEvent_t> ev((size_t) (nsteps * (nk + 1)));
+   for (auto &e : ev) CK(cudaEventCreate(&e));
+   std::vector<double> acc(nk, 0.);
+   gpe_status st = GPE_OK;
+   for (long c = 0; c < nsteps && st == GPE_OK; c++) {
+      cudaEvent_t *base = ev.data() + c * (nk + 1);
+      cudaEventRecord(base[0], s->st);
+      s->prof_ev = base + 1;
+      s->prof_i = 0;
+      s->prof_cap = nk;
+      st = DISPATCH(s, step(s, g, gd, nullptr));
+      s->prof_ev = nullptr;
+   }
+   if (st == GPE_OK && !s->cplx) st = DISPATCH(s, apply_scale(s));
+   cudaError_t e = cudaStreamSynchronize(s->st);
+   if (st == GPE_OK && e != cudaSuccess) st = fail(GPE_ERR_CUDA, cudaGetErrorString(e));
+   if (st == GPE_OK) {
+      for (long c = 0; c < nsteps; c++) {
+         cudaEvent_t *base = ev.data() + c * (nk + 1);
+         for (int i = 0; i < nk; i++) {
+            float f = 0.f;
+            cudaEventElapsedTime(&f, base[i], base[i + 1]);
+            acc[i] += f;
+         }
+      }
+      for (int i = 0; i < nk; i++) ms[i] = acc[i] / (double) nsteps;
+      if (count) *count = nk;
+   }
+   for (auto &x : ev) cudaEventDestroy(x);
+   return st;
+}

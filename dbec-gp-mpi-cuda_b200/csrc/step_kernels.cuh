@@ -1,0 +1,469 @@
+// step_kernels.cuh -- kernels of the split step (dipolar convolution passes,
+// fused calcnu + sweeps, norm) and of the observables.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace gpe {
+
+// ===========================================================================
+// Dipolar convolution phi = IFFT[Udd * FFT[|psi|^2]] (calcpsidd2_mem,
+// imag3d-mpicuda.cu:1460-1510) as five FFT passes over the half spectrum.
+// ===========================================================================
+
+// Pass 1: |psi|^2 rows -> half spectrum along z.  Two real rows form one
+// complex line (x_a + i x_b); after the FFT the two half spectra are split
+// with X_a = (Z_k + conj Z_{n-k})/2, X_b = (Z_k - conj Z_{n-k})/(2i).
+template <class R, bool CPLX>
+__global__ void __launch_bounds__(256) k_zfwd(const typename Tr<R, CPLX>::P *__restrict__ psi,
+                                              cpx<R> *__restrict__ spec, Dims d, FftPlan pz,
+                                              const cpx<R> *__restrict__ twz, int NP) {
+   using C = cpx<R>;
+   extern __shared__ __align__(16) unsigned char smem_raw[];
+   const int nz = d.nz, ls = nz + 2;
+   C *bufA = (C *) smem_raw;
+   C *bufB = bufA + NP * ls;
+   C *tw = bufB + NP * ls;
+   for (int i = threadIdx.x; i < nz; i += blockDim.x) tw[i] = twz[i];
+   const long long r0 = (long long) blockIdx.x * (2 * NP);
+   for (int e = threadIdx.x; e < 2 * NP * nz; e += blockDim.x) {
+      const int rr = e / nz, k = e - rr * nz;
+      const long long row = r0 + rr;
+      R v = (R) 0;
+      if (row < d.nxy) v = dens2(psi[row * nz + k]);
+      C *slot = &bufA[(rr >> 1) * ls + k];
+      if (rr & 1) slot->y = v; else slot->x = v;
+   }
+   __syncthreads();
+   C *res = fft_lines<C, false, true>(bufA, bufB, pz, NP, ls, 1, tw);
+   const int nzh = d.nzh;
+   for (int e = threadIdx.x; e < 2 * NP * nzh; e += blockDim.x) {
+      const int k = e / (2 * NP), rr = e - k * (2 * NP);
+      const long long row = r0 + rr;
+      if (row >= d.nxy) continue;
+      const C *line = res + (rr >> 1) * ls;
+      C Z = line[k];
+      C Zc = cconj(line[k == 0 ? 0 : nz - k]);
+      C X;
+      if (rr & 1) {
+         C t = csub(Z, Zc);
+         X = mk<R>(t.y * (R) 0.5, -t.x * (R) 0.5);
+      } else {
+         C t = cadd(Z, Zc);
+         X = mk<R>(t.x * (R) 0.5, t.y * (R) 0.5);
+      }
+      spec[(long long) k * d.nxy + row] = X;
+   }
+}
+
+// Passes 2 and 4: FFT along y; lines are contiguous (spec[(k nx + x) ny + y]).
+template <class R, bool INV>
+__global__ void __launch_bounds__(256) k_yfft(cpx<R> *__restrict__ spec, Dims d, FftPlan py,
+                                              const cpx<R> *__restrict__ twy, int LY) {
+   using C = cpx<R>;
+   extern __shared__ __align__(16) unsigned char smem_raw[];
+   const int ny = d.ny;
+   C *bufA = (C *) smem_raw;
+   C *bufB = bufA + LY * ny;
+   C *tw = bufB + LY * ny;
+   for (int i = threadIdx.x; i < ny; i += blockDim.x) tw[i] = twy[i];
+   const long long nlines = (long long) d.nzh * d.nx;
+   const long long l0 = (long long) blockIdx.x * LY;
+   const int nl = (int) ((nlines - l0) < LY ? (nlines - l0) : LY);
+   const C *src = spec + l0 * ny;
+   for (int e = threadIdx.x; e < nl * ny; e += blockDim.x) bufA[e] = src[e];
+   for (int e = nl * ny + threadIdx.x; e < LY * ny; e += blockDim.x) bufA[e] = mk<R>(0, 0);
+   __syncthreads();
+   C *res = fft_lines<C, INV, true>(bufA, bufB, py, LY, ny, 1, tw);
+   C *dst = spec + l0 * ny;
+   for (int e = threadIdx.x; e < nl * ny; e += blockDim.x) dst[e] = res[e];
+}
+
+// Pass 3: FFT along x, multiply by Udd(k) * scale^2, inverse FFT along x.
+// A CTA takes W consecutive y columns of one kz plane (interleaved layout:
+// element (column c, x) at x * W + c).
+template <class R>
+__global__ void __launch_bounds__(256) k_xconv(cpx<R> *__restrict__ spec, Dims d, FftPlan px,
+                                               const cpx<R> *__restrict__ twx, const double *__restrict__ udd,
+                                               const State *__restrict__ st, int W) {
+   using C = cpx<R>;
+   extern __shared__ __align__(16) unsigned char smem_raw[];
+   const int nx = d.nx, ny = d.ny;
+   C *bufA = (C *) smem_raw;
+   C *bufB = bufA + nx * W;
+   C *tw = bufB + nx * W;
+   for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = twx[i];
+   const int nyb = (ny + W - 1) / W;
+   const int kz = blockIdx.x / nyb;
+   const int y0 = (blockIdx.x - kz * nyb) * W;
+   C *plane = spec + (long long) kz * d.nxy;
+   for (int e = threadIdx.x; e < nx * W; e += blockDim.x) {
+      const int x = e / W, c = e - x * W;
+      const int y = y0 + c;
+      bufA[e] = (y < ny) ? plane[(long long) x * ny + y] : mk<R>(0, 0);
+   }
+   __syncthreads();
+   C *res = fft_lines<C, false, false>(bufA, bufB, px, W, 1, W, tw);
+   C *oth = (res == bufA) ? bufB : bufA;
+   const double s2 = st->scale2;
+   const int nxh = nx / 2 + 1, nyh = ny / 2 + 1;
+   const double *uplane = udd + (long long) kz * nxh * nyh;
+   for (int e = threadIdx.x; e < nx * W; e += blockDim.x) {
+      const int x = e / W, c = e - x * W;
+      int y = y0 + c;
+      if (y >= ny) y = ny - 1;
+      const int ax = (x <= nx / 2) ? x : nx - x;
+      const int ay = (y <= ny / 2) ? y : ny - y;
+      const R u = (R) (uplane[ax * nyh + ay] * s2);
+      res[e] = cscale(res[e], u);
+   }
+   __syncthreads();
+   C *fin = fft_lines<C, true, false>(res, oth, px, W, 1, W, tw);
+   for (int e = threadIdx.x; e < nx * W; e += blockDim.x) {
+      const int x = e / W, c = e - x * W;
+      const int y = y0 + c;
+      if (y < ny) plane[(long long) x * ny + y] = fin[e];
+   }
+}
+
+// Pass 5: Hermitian inverse along z -> phi rows (two rows per complex line).
+template <class R>
+__global__ void __launch_bounds__(256) k_zinv(const cpx<R> *__restrict__ spec, R *__restrict__ phi, Dims d,
+                                              FftPlan pz, const cpx<R> *__restrict__ twz, int NP) {
+   using C = cpx<R>;
+   extern __shared__ __align__(16) unsigned char smem_raw[];
+   const int nz = d.nz, nzh = d.nzh, ls = nz + 2;
+   C *bufA = (C *) smem_raw;
+   C *bufB = bufA + NP * ls;
+   C *tw = bufB + NP * ls;
+   for (int i = threadIdx.x; i < nz; i += blockDim.x) tw[i] = twz[i];
+   const long long r0 = (long long) blockIdx.x * (2 * NP);
+   C *half = bufB;  // [2NP][nzh]
+   for (int e = threadIdx.x; e < 2 * NP * nzh; e += blockDim.x) {
+      const int k = e / (2 * NP), rr = e - k * (2 * NP);
+      const long long row = r0 + rr;
+      half[rr * nzh + k] = (row < d.nxy) ? spec[(long long) k * d.nxy + row] : mk<R>(0, 0);
+   }
+   __syncthreads();
+   for (int e = threadIdx.x; e < NP * nz; e += blockDim.x) {
+      const int p = e / nz, k = e - p * nz;
+      C a, b;
+      if (k < nzh) {
+         a = half[(2 * p) * nzh + k];
+         b = half[(2 * p + 1) * nzh + k];
+      } else {
+         a = cconj(half[(2 * p) * nzh + nz - k]);
+         b = cconj(half[(2 * p + 1) * nzh + nz - k]);
+      }
+      if (k == 0 || 2 * k == nz) { a.y = 0; b.y = 0; }
+      bufA[p * ls + k] = mk<R>(a.x - b.y, a.y + b.x);
+   }
+   __syncthreads();
+   C *res = fft_lines<C, true, true>(bufA, bufB, pz, NP, ls, 1, tw);
+   for (int e = threadIdx.x; e < 2 * NP * nz; e += blockDim.x) {
+      const int rr = e / nz, k = e - rr * nz;
+      const long long row = r0 + rr;
+      if (row >= d.nxy) continue;
+      const C v = res[(rr >> 1) * ls + k];
+      phi[row * nz + k] = (rr & 1) ? v.y : v.x;
+   }
+}
+
+// Boundary planes of phi at one rank (calcpsidd2_kernel2a/2b with last = 1,
+// imag3d-mpicuda.cu:1591-1625): x = nx-1 <- x = 0, y = ny-1 <- y = 0,
+// z = nz-1 <- z = 0, each excluding the other two last indices.  The read
+// and write sets are disjoint, so all three copies run concurrently.
+template <class R>
+__global__ void k_phifix(R *__restrict__ phi, Dims d) {
+   const long long A = (long long) (d.ny - 1) * (d.nz - 1);
+   const long long B = (long long) (d.nx - 1) * (d.nz - 1);
+   const long long Cn = (long long) (d.nx - 1) * (d.ny - 1);
+   const long long tot = A + B + Cn;
+   for (long long e = blockIdx.x * (long long) blockDim.x + threadIdx.x; e < tot; e += (long long) gridDim.x * blockDim.x) {
+      if (e < A) {
+         const long long j = e / (d.nz - 1), k = e - j * (d.nz - 1);
+         phi[((long long) (d.nx - 1) * d.ny + j) * d.nz + k] = phi[j * d.nz + k];
+      } else if (e < A + B) {
+         const long long q = e - A, i = q / (d.nz - 1), k = q - i * (d.nz - 1);
+         phi[(i * d.ny + d.ny - 1) * d.nz + k] = phi[(i * d.ny) * d.nz + k];
+      } else {
+         const long long q = e - A - B, i = q / (d.ny - 1), j = q - i * (d.ny - 1);
+         phi[(i * d.ny + j) * d.nz + d.nz - 1] = phi[(i * d.ny + j) * d.nz];
+      }
+   }
+}
+
+// ===========================================================================
+// Sweeps.
+// ===========================================================================
+
+// calcnu fused into the x sweep: psi is read once, multiplied by the pending
+// 1/norm, advanced by the nonlinear/trap exponential and then swept along x
+// (calcnu_kernel imag3d-mpicuda.cu:1759 + calclux_kernel :1802).
+template <class R, bool CPLX, bool NU>
+__global__ void __launch_bounds__(128) k_xsweep(typename Tr<R, CPLX>::P *__restrict__ psi,
+                                                typename Tr<R, CPLX>::P *__restrict__ beta,
+                                                const R *__restrict__ phi, Dims d, Coef cx, Trap trap,
+                                                double g, double gd, double dt, const State *__restrict__ st) {
+   using P = typename Tr<R, CPLX>::P;
+   const long long line = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+   const long long nl = (long long) d.ny * d.nz;
+   if (line >= nl) return;
+   const int j = (int) (line / d.nz), k = (int) (line - (long long) j * d.nz);
+   const long long stx = nl;
+   const double scale = NU ? st->scale : 1.;
+   const R invN = (R) (1.0 / (double) d.npts);
+   P *ps = psi + line;
+   const R *ph = phi + line;
+   auto load = [&](int i) -> P {
+      P v = ps[(long long) i * stx];
+      if (NU) {
+         v = scl(v, scale);
+         v = nu_op<R>(v, ph[(long long) i * stx], (R) trap.v(i, j, k), (R) g, (R) gd, (R) dt, invN);
+      }
+      return v;
+   };
+   thomas_line<R, CPLX, false>(ps, beta + line, stx, d.nx, cx, load, 0.);
+}
+
+template <class R, bool CPLX>
+__global__ void __launch_bounds__(128) k_ysweep(typename Tr<R, CPLX>::P *__restrict__ psi,
+                                                typename Tr<R, CPLX>::P *__restrict__ beta, Dims d, Coef cy) {
+   using P = typename Tr<R, CPLX>::P;
+   const long long line = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+   if (line >= (long long) d.nx * d.nz) return;
+   const long long i = line / d.nz, k = line - i * d.nz;
+   const long long base = i * d.ny * d.nz + k;
+   P *ps = psi + base;
+   auto load = [&](int jj) -> P { return ps[(long long) jj * d.nz]; };
+   thomas_line<R, CPLX, false>(ps, beta + base, d.nz, d.ny, cy, load, 0.);
+}
+
+// z sweep; with SIMP each row also yields its Simpson integral of |psi|^2
+// (simpint3d_kernel, diffint.cu:106) for the norm.
+template <class R, bool CPLX, bool SIMP>
+__global__ void __launch_bounds__(128) k_zsweep(typename Tr<R, CPLX>::P *__restrict__ psi,
+                                                typename Tr<R, CPLX>::P *__restrict__ beta, Dims d, Coef cz,
+                                                double *__restrict__ rowsum, double hz) {
+   using P = typename Tr<R, CPLX>::P;
+   const long long row = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+   if (row >= d.nxy) return;
+   P *ps = psi + row * d.nz;
+   auto load = [&](int kk) -> P { return ps[kk]; };
+   double s = thomas_line<R, CPLX, SIMP>(ps, beta + row * d.nz, 1, d.nz, cz, load, hz);
+   if (SIMP) rowsum[row] = s;
+}
+
+// Standalone calcnu (operator-level entry point).
+template <class R, bool CPLX>
+__global__ void k_calcnu(typename Tr<R, CPLX>::P *__restrict__ psi, const R *__restrict__ phi, Dims d, Trap trap,
+                         double g, double gd, double dt) {
+   const R invN = (R) (1.0 / (double) d.npts);
+   for (long long q = blockIdx.x * (long long) blockDim.x + threadIdx.x; q < d.npts; q += (long long) gridDim.x * blockDim.x) {
+      const int k = (int) (q % d.nz);
+      const long long r = q / d.nz;
+      const int j = (int) (r % d.ny), i = (int) (r / d.ny);
+      psi[q] = nu_op<R>(psi[q], phi[q], (R) trap.v(i, j, k), (R) g, (R) gd, (R) dt, invN);
+   }
+}
+
+// ===========================================================================
+// Reductions.
+// ===========================================================================
+
+// Per-row Simpson of |psi|^2 along z (no sweep).
+template <class R, bool CPLX>
+__global__ void k_rows_dens(const typename Tr<R, CPLX>::P *__restrict__ psi, Dims d, double hz,
+                            double *__restrict__ rowA, double *__restrict__ rowB, const double *__restrict__ z2) {
+   const long long row = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+   if (row >= d.nxy) return;
+   const auto *ps = psi + row * d.nz;
+   Simpson a, b;
+   a.init(d.nz);
+   b.init(d.nz);
+   for (int k = 0; k < d.nz; k++) {
+      const double f = (double) dens2(ps[k]);
+      a.add(k, f);
+      if (rowB) b.add(k, z2[k] * f);
+   }
+   rowA[row] = a.finish(hz);
+   if (rowB) rowB[row] = b.finish(hz);
+}
+
+// norm = sqrt(S_x S_y rowsum) (calcnorm, imag3d-mpicuda.cu:1194-1218), stores
+// norm, scale = 1/norm and scale^2 in the state.
+__global__ void k_norm_final(const double *__restrict__ rowsum, Dims d, double hx, double hy, State *st,
+                             double *out_norm) {
+   extern __shared__ double tx[];
+   for (int i = threadIdx.x; i < d.nx; i += blockDim.x) tx[i] = simpint_arr(hy, rowsum + (long long) i * d.ny, d.ny);
+   __syncthreads();
+   if (threadIdx.x == 0) {
+      const double nrm = sqrt(simpint_arr(hx, tx, d.nx));
+      const double t = 1. / nrm;
+      st->norm = nrm;
+      st->scale = t;
+      st->scale2 = t * t;
+      if (out_norm) *out_norm = nrm;
+   }
+}
+
+// psi *= scale (calcnorm_kernel, imag3d-mpicuda.cu:1220-1233).
+template <class R, bool CPLX>
+__global__ void k_apply_scale(typename Tr<R, CPLX>::P *__restrict__ psi, long long n, const State *__restrict__ st) {
+   const double s = st->scale;
+   for (long long q = blockIdx.x * (long long) blockDim.x + threadIdx.x; q < n; q += (long long) gridDim.x * blockDim.x)
+      psi[q] = scl(psi[q], s);
+}
+
+__global__ void k_state_set(State *st, double scale) {
+   st->scale = scale;
+   st->scale2 = scale * scale;
+}
+
+// rms sizes from per-row sums A = S_z |psi|^2, B = S_z z^2 |psi|^2
+// (calcrms, imag3d-mpicuda.cu:1639-1685).
+__global__ void k_rms_final(const double *__restrict__ rowA, const double *__restrict__ rowB, Dims d, double hx,
+                            double hy, const double *__restrict__ x2, const double *__restrict__ y2,
+                            double *__restrict__ out) {
+   extern __shared__ double sm[];
+   double *ta = sm, *tb = sm + d.nx, *tc = sm + 2 * d.nx;
+   for (int i = threadIdx.x; i < d.nx; i += blockDim.x) {
+      const double *ra = rowA + (long long) i * d.ny;
+      const double *rb = rowB + (long long) i * d.ny;
+      ta[i] = x2[i] * simpint_arr(hy, ra, d.ny);
+      tb[i] = simpint_arr(hy, rb, d.ny);
+      // y^2-weighted: Simpson of y2[j] * A[i][j] in the reference's order
+      double sumi = 0., sumj = 0., sumk = 0.;
+      const long N = d.ny;
+      for (long c = 1; c < N - 1; c += 2) {
+         sumi += y2[c] * ra[c];
+         sumj += y2[c - 1] * ra[c - 1];
+         sumk += y2[c + 1] * ra[c + 1];
+      }
+      double sum = sumj + 4. * sumi + sumk;
+      if (N % 2 == 0) sum += (5. * y2[N - 1] * ra[N - 1] + 8. * y2[N - 2] * ra[N - 2] - y2[N - 3] * ra[N - 3]) / 4.;
+      tc[i] = sum * hy / 3.;
+   }
+   __syncthreads();
+   if (threadIdx.x == 0) {
+      const double rx = sqrt(simpint_arr(hx, ta, d.nx));
+      const double ry = sqrt(simpint_arr(hx, tc, d.nx));
+      const double rz = sqrt(simpint_arr(hx, tb, d.nx));
+      out[1] = rx;
+      out[2] = ry;
+      out[3] = rz;
+      out[0] = sqrt(rx * rx + ry * ry + rz * rz);
+   }
+}
+
+// Generic S_x S_y of a per-row array (mu, E, norm).
+__global__ void k_xy_final(const double *__restrict__ rowA, Dims d, double hx, double hy, double *__restrict__ out) {
+   extern __shared__ double tx[];
+   for (int i = threadIdx.x; i < d.nx; i += blockDim.x) tx[i] = simpint_arr(hy, rowA + (long long) i * d.ny, d.ny);
+   __syncthreads();
+   if (threadIdx.x == 0) *out = simpint_arr(hx, tx, d.nx);
+}
+
+// 4th-order first derivative with the reference's edge rules
+// (calcmuen_kernel1x/1y/1z, imag3d-mpicuda.cu:1293-1422).
+template <class F>
+__device__ __forceinline__ double fd4(F f, int i, int n, double h) {
+   if (i == 0 || i == n - 1) return 0.;
+   if (i == 1) return (f(2) - f(0)) / (2. * h);
+   if (i == n - 2) return (f(n - 1) - f(n - 3)) / (2. * h);
+   return (f(i - 2) - 8. * f(i - 1) + 8. * f(i + 1) - f(i + 2)) / (12. * h);
+}
+
+// Per-row Simpson of the mu and E integrands (calcmuen_kernel2,
+// imag3d-mpicuda.cu:1424-1450); real time differentiates |psi| (real:1401).
+template <class R, bool CPLX>
+__global__ void k_muen_rows(const typename Tr<R, CPLX>::P *__restrict__ psi, const R *__restrict__ phi, Dims d,
+                            Trap trap, double g, double gd, double dx, double dy, double dz, double par,
+                            double *__restrict__ rowMu, double *__restrict__ rowEn) {
+   const long long row = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+   if (row >= d.nxy) return;
+   const int i = (int) (row / d.ny), j = (int) (row - (long long) i * d.ny);
+   const long long sx = (long long) d.ny * d.nz, sy = d.nz;
+   const auto *base = psi + row * d.nz;
+   const double invN = 1.0 / (double) d.npts;
+   auto amp = [&](const typename Tr<R, CPLX>::P &v) -> double {
+      if (CPLX) return sqrt((double) dens2(v));
+      return (double) *(const R *) &v;
+   };
+   Simpson smu, sen;
+   smu.init(d.nz);
+   sen.init(d.nz);
+   for (int k = 0; k < d.nz; k++) {
+      const auto *pk = base + k;
+      const double ddx = fd4([&](int q) { return amp(pk[(long long) (q - i) * sx]); }, i, d.nx, dx);
+      const double ddy = fd4([&](int q) { return amp(pk[(long long) (q - j) * sy]); }, j, d.ny, dy);
+      const double ddz = fd4([&](int q) { return amp(base[q]); }, k, d.nz, dz);
+      double dpsi = (ddx * ddx) / (3. - par);
+      dpsi += (ddy * ddy) / (3. - par);
+      dpsi += (ddz * ddz) / (3. - par);
+      const double psi2 = (double) dens2(*pk);
+      const double psi2lin = psi2 * g;
+      const double psidd2lin = ((double) phi[row * d.nz + k] * invN) * gd;
+      const double tmppot = trap.v(i, j, k);
+      smu.add(k, (tmppot + psi2lin + psidd2lin) * psi2 + dpsi);
+      sen.add(k, (tmppot + 0.5 * psi2lin + 0.5 * psidd2lin) * psi2 + dpsi);
+   }
+   rowMu[row] = smu.finish(dz);
+   rowEn[row] = sen.finish(dz);
+}
+
+// ---- density outputs -------------------------------------------------------
+// Line integral of |psi|^2 along `axis` for every line; out is indexed by the
+// two remaining axes in (x, y, z) order.
+template <class R, bool CPLX>
+__global__ void k_lineint_psi(const typename Tr<R, CPLX>::P *__restrict__ psi, Dims d, int axis, double h,
+                              double *__restrict__ out) {
+   const int n[3] = {d.nx, d.ny, d.nz};
+   const long long s[3] = {(long long) d.ny * d.nz, d.nz, 1};
+   const int a1 = axis == 0 ? 1 : 0, a2 = axis == 2 ? 1 : 2;
+   const long long nl = (long long) n[a1] * n[a2];
+   const long long l = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+   if (l >= nl) return;
+   const long long u = l / n[a2], v = l - u * n[a2];
+   const auto *p = psi + u * s[a1] + v * s[a2];
+   Simpson sp;
+   sp.init(n[axis]);
+   for (int c = 0; c < n[axis]; c++) sp.add(c, (double) dens2(p[(long long) c * s[axis]]));
+   out[l] = sp.finish(h);
+}
+
+// out[u] = Simpson along axis `ax` (0 rows, 1 columns) of a [n0][n1] array.
+__global__ void k_lineint_arr(const double *__restrict__ a, int n0, int n1, int ax, double h, double *__restrict__ out) {
+   const int l = blockIdx.x * blockDim.x + threadIdx.x;
+   if (ax == 1) {
+      if (l < n0) out[l] = simpint_arr(h, a + (long long) l * n1, n1, 1);
+   } else {
+      if (l < n1) out[l] = simpint_arr(h, a + l, n0, n1);
+   }
+}
+
+// |psi|^2 gathered on a strided sub-grid of a box (3D cuts and raw density).
+template <class R, bool CPLX>
+__global__ void k_gather_dens(const typename Tr<R, CPLX>::P *__restrict__ psi, Dims d, int i0, int i1, int si,
+                              int j0, int j1, int sj, int k0, int k1, int sk, double *__restrict__ out) {
+   const long long ni = (i1 - i0 + si - 1) / si, nj = (j1 - j0 + sj - 1) / sj, nk = (k1 - k0 + sk - 1) / sk;
+   const long long tot = ni * nj * nk;
+   for (long long e = blockIdx.x * (long long) blockDim.x + threadIdx.x; e < tot; e += (long long) gridDim.x * blockDim.x) {
+      const long long a = e / (nj * nk), r = e - a * nj * nk, b = r / nk, c = r - b * nk;
+      const long long i = i0 + a * si, j = j0 + b * sj, k = k0 + c * sk;
+      out[e] = (double) dens2(psi[(i * d.ny + j) * d.nz + k]);
+   }
+}
+
+template <class R, bool CPLX>
+__global__ void k_init_density(typename Tr<R, CPLX>::P *__restrict__ psi, const double *__restrict__ rho, long long n) {
+   using P = typename Tr<R, CPLX>::P;
+   for (long long q = blockIdx.x * (long long) blockDim.x + threadIdx.x; q < n; q += (long long) gridDim.x * blockDim.x) {
+      const double a = sqrt(rho[q]);
+      P v = zero_of<P>();
+      if constexpr (CPLX) v.x = (R) a; else v = (R) a;
+      psi[q] = v;
+   }
+}
+
+}  // namespace gpe

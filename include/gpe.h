@@ -1,0 +1,141 @@
+/*
+ * gpe.h -- C ABI of the B200 (sm_100a) dipolar Gross-Pitaevskii solver.
+ *
+ * Drop-in for the hot path of DBEC-GP-MPI-CUDA's imag3d-mpicuda and
+ * real3d-mpicuda: the split-step Crank-Nicolson propagator in imaginary time
+ * (real FP64 psi, renormalised every step) and in real time (complex128 psi).
+ * The reference keeps its state in file-scope globals and exposes C functions
+ * on cudaPitchedPtr arguments (src/imag3d-mpicuda/imag3d-mpicuda.cuh:48-159);
+ * here every piece of device state is owned by a handle, so solvers are
+ * re-entrant and several can live in one process.
+ *
+ * Conventions
+ *  - Host arrays are x-major [nx][ny][nz] with z contiguous, as the reference
+ *    host tensors (src/utils/mem.c:104-130).  Complex psi is interleaved
+ *    (re, im) doubles like the reference's cuDoubleComplex tensor
+ *    (real3d-mpicuda.cu:40); page-locked buffers are copied without staging.
+ *  - Every call returns a gpe_status; the library never calls exit().
+ *    gpe_last_error() returns a thread-local message for the last failure.
+ *  - One host thread per handle.  Work is queued on the handle's stream
+ *    (the caller's cudaStream_t if one was given to gpe_create).
+ *  - The library owns all device memory; callers own host buffers.
+ */
+#ifndef GPE_H
+#define GPE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+   GPE_OK = 0,
+   GPE_ERR_PARAM = 1,       /* invalid argument or unsupported grid */
+   GPE_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+   GPE_ERR_OOM = 3,         /* device allocation failed */
+   GPE_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up */
+   GPE_ERR_STATE = 5,       /* call not valid in the handle's state */
+   GPE_ERR_IO = 6,          /* file could not be read or written */
+   GPE_ERR_UNSUPPORTED = 7, /* feature not available in this build */
+   GPE_ERR_BUDGET = 8       /* admission refused by the memory budget */
+} gpe_status;
+
+enum { GPE_MODE_IMAG = 0, GPE_MODE_REAL = 1 };
+enum { GPE_PREC_FP64 = 0, GPE_PREC_MIXED = 1 };
+
+/* Density outputs, the reference's out* writers
+ * (src/imag3d-mpicuda/imag3d-mpicuda.cu:1944-2399). */
+enum {
+   GPE_DEN_1D_X = 0, GPE_DEN_1D_Y = 1, GPE_DEN_1D_Z = 2,
+   GPE_DEN_2D_XY = 3, GPE_DEN_2D_XZ = 4, GPE_DEN_2D_YZ = 5,
+   GPE_DEN_3D_XY0 = 6, GPE_DEN_3D_X0Z = 7, GPE_DEN_3D_0YZ = 8,
+   GPE_DEN_3D = 9
+};
+
+/* Physical and numerical parameters: the keys of readpar()
+ * (src/imag3d-mpicuda/imag3d-mpicuda.cu:650-829).  g and gd are not part of
+ * the handle; they are passed per run so that ramps and quenches follow the
+ * reference's phase loops exactly. */
+typedef struct {
+   int mode;         /* GPE_MODE_IMAG or GPE_MODE_REAL */
+   int precision;    /* GPE_PREC_FP64 or GPE_PREC_MIXED */
+   int opt;          /* OPTION: par = 2 if opt == 2, else 1 */
+   int device;       /* CUDA device, -1 = current (DEVICE key) */
+   long nx, ny, nz;  /* even, in [8, 1024], prime factors 2, 3 and 5 only */
+   double dx, dy, dz, dt;
+   double gamma, nu, lambda;
+   double cutoff;
+} gpe_params;
+
+typedef struct gpe_solver gpe_solver;
+
+/* Replaces initdevice() + the cudaMalloc3D calls of main()
+ * (imag3d-mpicuda.cu:103-176, 982-1154).  stream may be NULL. */
+gpe_status gpe_create(const gpe_params *p, void *stream, gpe_solver **out);
+void gpe_destroy(gpe_solver *s);
+const char *gpe_last_error(void);
+/* Device bytes the handle would allocate for these parameters. */
+gpe_status gpe_device_bytes(const gpe_params *p, long long *bytes);
+
+/* initpsi Gaussian (imag3d-mpicuda.cu:835-867, real3d-mpicuda.cu:914-923). */
+gpe_status gpe_init_gaussian(gpe_solver *s);
+/* real3d initpsi from imag3d-den.bin: psi = (sqrt(rho), 0)
+ * (real3d-mpicuda.cu:925-947); rho is a host [nx][ny][nz] array. */
+gpe_status gpe_init_density(gpe_solver *s, const double *rho);
+/* Host <-> device psi (the psiparam cudaMemcpy3D of imag3d-mpicuda.cu:226-236):
+ * nx*ny*nz doubles in imaginary time, 2*nx*ny*nz interleaved doubles in real
+ * time.  Both calls return when the copy has completed. */
+gpe_status gpe_set_psi(gpe_solver *s, const double *psi);
+gpe_status gpe_get_psi(gpe_solver *s, double *psi);
+
+/* calcnorm (imag3d-mpicuda.cu:1194-1233; real3d-mpicuda.cu:1304-1322).
+ * renormalize != 0 divides psi by the norm as imag3d does. */
+gpe_status gpe_calcnorm(gpe_solver *s, int renormalize, double *norm);
+/* The step loops of imag3d-mpicuda.cu:309-325,397-404,472-479 and
+ * real3d-mpicuda.cu:328-339,411-424,496-508.  Before each step
+ * *g += g_inc, *gd += gd_inc.  In imaginary time every step ends with the
+ * renormalisation and *last_norm (may be NULL) receives the last
+ * pre-renormalisation norm (left untouched when nsteps == 0 or in real
+ * time).  rms_every > 0 evaluates calcrms after every step whose index c
+ * satisfies c % rms_every == 0 (DYNAOUT, real3d:419-423)
+ * into rms_out[4 * (c / rms_every)]; rms_every <= 0 disables it. */
+gpe_status gpe_run(gpe_solver *s, long nsteps, double *g, double *gd, double g_inc, double gd_inc,
+                   double *last_norm, long rms_every, double *rms_out);
+/* calcmuen (imag3d-mpicuda.cu:1250-1450): mu and E, not divided by par. */
+gpe_status gpe_calcmuen(gpe_solver *s, double g, double gd, double *mu, double *en);
+/* calcrms (imag3d-mpicuda.cu:1639-1744): rms[0] = <r>, rms[1..3] = <x>,<y>,<z>. */
+gpe_status gpe_calcrms(gpe_solver *s, double *rms);
+/* |psi(Nx/2, Ny/2, Nz/2)|^2 (psiNx2Ny2Nz2param, imag3d-mpicuda.cu:231-236). */
+gpe_status gpe_psi_center2(gpe_solver *s, double *value);
+/* Density outputs (out* writers, imag3d-mpicuda.cu:1944-2399).  Writes the
+ * doubles the reference writes to the file (pairs, triples or raw 3D) into
+ * out (capacity cap doubles); *count receives the number written. */
+gpe_status gpe_density(gpe_solver *s, int kind, long outstpx, long outstpy, long outstpz,
+                       double *out, long cap, long *count);
+
+/* Operator-level entry points, one per reference routine, for parity tests. */
+gpe_status gpe_calcpsidd2(gpe_solver *s);               /* calcpsidd2_mem, imag3d:1460-1510 */
+gpe_status gpe_get_phi(gpe_solver *s, double *phi);     /* psidd2 real view [nx][ny][nz] */
+gpe_status gpe_calcnu(gpe_solver *s, double g, double gd); /* calcnu, imag3d:1752-1783 */
+gpe_status gpe_calclux(gpe_solver *s);                  /* calclux, imag3d:1790-1844 */
+gpe_status gpe_calcluy(gpe_solver *s);                  /* calcluy, imag3d:1851-1900 */
+gpe_status gpe_calcluz(gpe_solver *s);                  /* calcluz, imag3d:1907-1942 */
+gpe_status gpe_synchronize(gpe_solver *s);
+
+/* Kernel launches queued by this handle since creation (for accounting). */
+gpe_status gpe_launch_count(gpe_solver *s, long long *count);
+/* Step timing on the handle's stream: runs nsteps plain steps (fixed g, gd)
+ * bracketed by CUDA events and returns the elapsed milliseconds. */
+gpe_status gpe_time_steps(gpe_solver *s, long nsteps, double g, double gd, double *ms);
+/* Per-kernel timing: runs nsteps plain steps with a CUDA event around every
+ * kernel of the step and returns, per kernel of one step, the mean duration in
+ * milliseconds (ms[i], i < *count <= cap).  gpe_step_kernel_name(i) names
+ * kernel i, gpe_step_kernel_bytes(s, i) its algorithmic bytes per launch. */
+gpe_status gpe_profile_step(gpe_solver *s, long nsteps, double g, double gd, double *ms, int cap, int *count);
+const char *gpe_step_kernel_name(gpe_solver *s, int i);
+double gpe_step_kernel_bytes(gpe_solver *s, int i);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPE_H */
