@@ -28,7 +28,7 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
                   "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC]
 
 LIB_SOURCES = ["solver.cu"]
-LIB_DEPS = ["solver.cu", "common.cuh", "fft.cuh", "kernels.cuh", "step_kernels.cuh"]
+LIB_DEPS = ["solver.cu", "common.cuh", "fft.cuh", "kernels.cuh", "step_kernels.cuh", "sweep_kernels.cuh", "tma.cuh"]
 HOST_COMMON = ["cfg.cpp", "cli.cpp"]
 PROGRAMS = {"imag3d-mpicuda": "imag3d_main.cpp", "real3d-mpicuda": "real3d_main.cpp"}
 

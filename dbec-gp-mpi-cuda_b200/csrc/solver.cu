@@ -12,8 +12,11 @@
 #include <string>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "gpe.h"
 #include "step_kernels.cuh"
+#include "sweep_kernels.cuh"
 
 using namespace gpe;
 
@@ -27,12 +30,16 @@ static gpe_status fail(gpe_status st, const std::string &msg) {
    return st;
 }
 
+// On failure the runtime's last-error slot is cleared so that a non-sticky
+// error is reported once, by the call that caused it.
 #define CK(call)                                                                                   \
    do {                                                                                           \
       cudaError_t e_ = (call);                                                                    \
-      if (e_ != cudaSuccess)                                                                      \
+      if (e_ != cudaSuccess) {                                                                    \
+         (void) cudaGetLastError();                                                               \
          return fail(e_ == cudaErrorMemoryAllocation ? GPE_ERR_OOM : GPE_ERR_CUDA,                \
                      std::string(#call) + ": " + cudaGetErrorString(e_));                          \
+      }                                                                                           \
    } while (0)
 
 #define CKL()                                                                                      \
@@ -58,17 +65,28 @@ struct gpe_solver {
    FftPlan px{}, py{}, pz{};
    int NP = 1, LY = 1, WX = 1;
    size_t esz_psi = 8, esz_c = 16, esz_r = 8;
-   void *psi = nullptr, *beta = nullptr, *spec = nullptr, *phi = nullptr;
+   void *psi = nullptr, *spec = nullptr, *phi = nullptr;
    void *twx = nullptr, *twy = nullptr, *twz = nullptr;
    double *udd = nullptr;
    void *alpha[3] = {nullptr, nullptr, nullptr}, *gamma[3] = {nullptr, nullptr, nullptr};
    double2 A[3], A0r[3], mA[3];
    double *x2 = nullptr, *y2 = nullptr, *z2 = nullptr;
    double *rowA = nullptr, *rowB = nullptr, *tmp = nullptr, *obs = nullptr;
+   long long row_cap = 0;  // doubles in rowA / rowB: the largest of nx*ny, nx*nz, ny*nz
    State *state = nullptr;
    std::vector<double> hx, hy, hz, hx2, hy2, hz2;
    long long launches = 0;
    size_t obs_cap = 0;
+   // sweep configuration per axis (x, y: TMA tensor tiles; z: bulk rows)
+   struct Sweep {
+      int TW = 8, MSEG = 8, boxn = 0, nbox = 1, LS = 0;
+      size_t smem = 0;
+      CUtensorMap tm_psi{}, tm_phi{};
+      SegTab tab{};
+      void *M = nullptr, *N = nullptr;
+   } sw[3];
+   double *wz = nullptr;      // Simpson weights along z (norm partials)
+   uint32_t *err = nullptr;   // device status word (bounded waits)
    // per-kernel profiling: when prof_ev is set, mark() records an event
    // after every kernel of a step
    cudaEvent_t *prof_ev = nullptr;
@@ -109,6 +127,8 @@ static gpe_status validate(const gpe_params *p) {
    }
    if (!(p->dx > 0 && p->dy > 0 && p->dz > 0 && p->dt > 0)) return fail(GPE_ERR_PARAM, "DX, DY, DZ, DT must be positive");
    if (!(p->cutoff > 0)) return fail(GPE_ERR_PARAM, "CUTOFF must be positive");
+   if (p->precision == GPE_PREC_MIXED && p->mode == GPE_MODE_IMAG && p->nz % 4)
+      return fail(GPE_ERR_PARAM, "mixed precision in imaginary time needs NZ divisible by 4 (16-byte rows)");
    return GPE_OK;
 }
 
@@ -123,11 +143,11 @@ extern "C" gpe_status gpe_device_bytes(const gpe_params *p, long long *bytes) {
    const long long nzh = p->nz / 2 + 1;
    const size_t r = (p->precision == GPE_PREC_MIXED) ? 4 : 8;
    long long b = 0;
-   b += 2 * npts * (long long) psi_esz(p);               // psi + beta
+   b += npts * (long long) psi_esz(p);                   // psi
    b += nzh * p->nx * p->ny * (long long) (2 * r);       // spectrum
    b += npts * (long long) r;                            // phi
    b += nzh * (p->nx / 2 + 1) * (p->ny / 2 + 1) * 8;     // Udd octant
-   b += 4 * p->nx * p->ny * 8;                           // row sums
+   b += 4 * std::max(p->nx * p->ny, std::max(p->nx * p->nz, p->ny * p->nz)) * 8;  // row sums
    b += 1 << 20;                                         // tables, state
    if (bytes) *bytes = b;
    return GPE_OK;
@@ -191,6 +211,154 @@ static gpe_status make_coef(gpe_solver *s, int ax, long n, double d2) {
    return GPE_OK;
 }
 
+// Segment tables of the parallel Thomas sweep of axis ax (line length n,
+// segment length m, P segments; the last segment ends at n-3):
+//   M[i] = prod_{j=i+1}^{H_p+1} gamma[j] A   for i in segment p < P-1
+//   N[k] = prod_{j=lo_p}^{k-1} alpha[j]       for k in (lo_p, hf_p + 1]
+// computed in long double and rounded once.
+static gpe_status make_segtab(gpe_solver *s, int ax, long n, double d2, int m, int P) {
+   typedef std::complex<long double> Z;
+   const long double c = (long double) s->p.dt / (long double) d2 / (3.L - (long double) s->par);
+   Z A0, A;
+   if (!s->cplx) { A0 = 1.L + c; A = -0.5L * c; }
+   else { A0 = Z(1.L, c); A = Z(0.L, -0.5L * c); }
+   // coefficients as uploaded (double), promoted: the tables multiply exactly those
+   std::vector<Z> al(n - 1), ga(n - 1);
+   {
+      std::vector<double> ad((size_t) (s->cplx ? 2 : 1) * (n - 1)), gd((size_t) (s->cplx ? 2 : 1) * (n - 1));
+      CK(cudaMemcpy(ad.data(), s->alpha[ax], sizeof(double) * ad.size(), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(gd.data(), s->gamma[ax], sizeof(double) * gd.size(), cudaMemcpyDeviceToHost));
+      for (long i = 0; i < n - 1; i++) {
+         al[i] = s->cplx ? Z(ad[2 * i], ad[2 * i + 1]) : Z(ad[i], 0.L);
+         ga[i] = s->cplx ? Z(gd[2 * i], gd[2 * i + 1]) : Z(gd[i], 0.L);
+      }
+      const double2 Ad = s->A[ax];
+      A = Z(Ad.x, Ad.y);
+   }
+   std::vector<Z> M(n, Z(0)), N(n, Z(0));
+   for (int p = 0; p < P; p++) {
+      const long lo = (long) p * m;
+      const bool top = p == P - 1;
+      const long hf = top ? n - 3 : lo + m - 1;
+      if (!top) {
+         Z r = 1;
+         for (long i = hf; i >= lo; i--) { r *= ga[i + 1] * A; M[i] = r; }
+      }
+      Z r = 1;
+      for (long i = lo; i <= hf; i++) { r *= al[i]; N[i + 1] = r; }
+   }
+   if (!s->cplx) {
+      std::vector<double> a(n), b(n);
+      for (long i = 0; i < n; i++) { a[i] = (double) M[i].real(); b[i] = (double) N[i].real(); }
+      CKS(upload(&s->sw[ax].M, a.data(), n));
+      CKS(upload(&s->sw[ax].N, b.data(), n));
+   } else {
+      std::vector<double2> a(n), b(n);
+      for (long i = 0; i < n; i++) {
+         a[i] = make_double2((double) M[i].real(), (double) M[i].imag());
+         b[i] = make_double2((double) N[i].real(), (double) N[i].imag());
+      }
+      CKS(upload(&s->sw[ax].M, a.data(), n));
+      CKS(upload(&s->sw[ax].N, b.data(), n));
+   }
+   SegTab &t = s->sw[ax].tab;
+   t.al = s->alpha[ax];
+   t.ga = s->gamma[ax];
+   t.M = s->sw[ax].M;
+   t.N = s->sw[ax].N;
+   t.A = s->A[ax];
+   t.A0r = s->A0r[ax];
+   t.mA = s->mA[ax];
+   t.n = (int) n;
+   t.m = m;
+   t.P = P;
+   return GPE_OK;
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static gpe_status encoder(EncodeTiledFn *fn) {
+   static EncodeTiledFn cached = nullptr;
+   if (!cached) {
+      void *f = nullptr;
+      cudaDriverEntryPointQueryResult q;
+      CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q));
+      if (!f || q != cudaDriverEntryPointSuccess) return fail(GPE_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
+      cached = (EncodeTiledFn) f;
+   }
+   *fn = cached;
+   return GPE_OK;
+}
+
+// 3D tensor map over a [nx][ny][w * nz] array of `esz`-byte scalars with box
+// {bw, by, bx} (innermost first).
+static gpe_status make_tmap(CUtensorMap *m, void *base, size_t esz, long w_nz, long ny, long nx, int bw, int by, int bx) {
+   EncodeTiledFn enc;
+   CKS(encoder(&enc));
+   cuuint64_t dims[3] = {(cuuint64_t) w_nz, (cuuint64_t) ny, (cuuint64_t) nx};
+   cuuint64_t strides[2] = {(cuuint64_t) (w_nz * esz), (cuuint64_t) (w_nz * esz * ny)};
+   cuuint32_t box[3] = {(cuuint32_t) bw, (cuuint32_t) by, (cuuint32_t) bx};
+   cuuint32_t es[3] = {1, 1, 1};
+   CUresult r = enc(m, esz == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims,
+                    strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+   if (r != CUDA_SUCCESS) return fail(GPE_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int) r) + ")");
+   return GPE_OK;
+}
+
+// Lines per CTA and segment length for a sweep over lines of length n with
+// `tw_base` lines filling a 128-byte row: at most 256 threads per CTA.
+static void pick_sweep(int n, int tw_base, int &TW, int &MSEG, int &P) {
+   const int ms[2] = {8, 16};
+   for (int tw = tw_base; tw >= 2; tw /= 2)
+      for (int mi = 0; mi < 2; mi++) {
+         const int p = (n - 2 + ms[mi] - 1) / ms[mi];
+         if (tw * p <= 256) { TW = tw; MSEG = ms[mi]; P = p; return; }
+      }
+   TW = 2; MSEG = 16; P = (n - 2 + 15) / 16;
+}
+
+static gpe_status setup_sweeps(gpe_solver *s) {
+   const Dims &d = s->d;
+   const size_t esz = s->esz_psi, rsz = s->esz_r;
+   const int E = s->cplx ? 2 : 1;
+   const int tw_base = (int) (128 / esz);
+   const long nn[3] = {d.nx, d.ny, d.nz};
+   const double h2[3] = {s->p.dx * s->p.dx, s->p.dy * s->p.dy, s->p.dz * s->p.dz};
+   for (int ax = 0; ax < 3; ax++) {
+      auto &w = s->sw[ax];
+      int P = 1;
+      pick_sweep((int) nn[ax], tw_base, w.TW, w.MSEG, P);
+      CKS(make_segtab(s, ax, nn[ax], h2[ax], w.MSEG, P));
+      const size_t carry = 2 * (size_t) P * w.TW * esz;
+      if (ax < 2) {
+         w.boxn = (int) std::min<long>(nn[ax], 256);
+         w.nbox = (int) ((nn[ax] + w.boxn - 1) / w.boxn);
+         const long rows = (long) w.boxn * w.nbox;
+         const int by = ax == 1 ? w.boxn : 1, bx = ax == 0 ? w.boxn : 1;
+         CKS(make_tmap(&w.tm_psi, s->psi, s->fp32 ? 4 : 8, E * d.nz, d.ny, d.nx, E * w.TW, by, bx));
+         CKS(make_tmap(&w.tm_phi, s->phi, rsz, d.nz, d.ny, d.nx, w.TW, by, bx));
+         w.smem = 128 + rows * w.TW * esz + (ax == 0 ? rows * w.TW * rsz : 0) + 16 + carry;
+      } else {
+         w.LS = (int) (d.nz + 16 / esz);
+         w.smem = 128 + (size_t) w.TW * w.LS * esz + carry + (size_t) P * w.TW * sizeof(double);
+      }
+   }
+   // Simpson weights along z: sum_k wz[k] f[k] * dz / 3 equals simpint (diffint.cu:37-66)
+   std::vector<double> wz(d.nz, 0.);
+   const int N = d.nz, mm = (N % 2) ? N : N - 1;
+   for (int k = 0; k < mm; k++) wz[k] = (k == 0 || k == mm - 1) ? 1. : ((k % 2) ? 4. : 2.);
+   if (N % 2 == 0) { wz[N - 1] += 5. / 4.; wz[N - 2] += 8. / 4.; wz[N - 3] -= 1. / 4.; }
+   void *t = nullptr;
+   CKS(upload(&t, wz.data(), wz.size()));
+   s->wz = (double *) t;
+   CK(cudaMalloc(&s->err, sizeof(uint32_t)));
+   CK(cudaMemset(s->err, 0, sizeof(uint32_t)));
+   return GPE_OK;
+}
+
 // initpotdd (imag3d-mpicuda.cu:945-980) on the octant |kx| <= nx/2,
 // |ky| <= ny/2, kz <= nz/2: Udd depends on kx^2, ky^2, kz^2 only, and the
 // squares of the reference's negative k values equal those of the octant.
@@ -220,14 +388,18 @@ static gpe_status make_udd(gpe_solver *s) {
 }
 
 static void free_all(gpe_solver *s) {
-   void *ptrs[] = {s->psi, s->beta, s->spec, s->phi, s->twx, s->twy, s->twz, s->udd, s->x2, s->y2, s->z2,
+   void *ptrs[] = {s->psi, s->spec, s->phi, s->twx, s->twy, s->twz, s->udd, s->x2, s->y2, s->z2,
                    s->rowA, s->rowB, s->tmp, s->obs, s->state};
    for (void *q : ptrs)
       if (q) cudaFree(q);
    for (int a = 0; a < 3; a++) {
       if (s->alpha[a]) cudaFree(s->alpha[a]);
       if (s->gamma[a]) cudaFree(s->gamma[a]);
+      if (s->sw[a].M) cudaFree(s->sw[a].M);
+      if (s->sw[a].N) cudaFree(s->sw[a].N);
    }
+   if (s->wz) cudaFree(s->wz);
+   if (s->err) cudaFree(s->err);
    if (s->own_stream && s->st) cudaStreamDestroy(s->st);
 }
 
@@ -262,12 +434,12 @@ static gpe_status create_impl(const gpe_params *p, void *stream, gpe_solver *s) 
    s->WX = std::max(4, std::min(16, floor_pow2(std::max(1LL, budget / (long long) (2 * d.nx * s->esz_c)))));
 
    CK(cudaMalloc(&s->psi, s->esz_psi * d.npts));
-   CK(cudaMalloc(&s->beta, s->esz_psi * d.npts));
    CK(cudaMalloc(&s->spec, s->esz_c * (size_t) d.nzh * d.nxy));
    CK(cudaMalloc(&s->phi, r * d.npts));
    CK(cudaMemset(s->psi, 0, s->esz_psi * d.npts));
-   CK(cudaMalloc(&s->rowA, sizeof(double) * d.nxy));
-   CK(cudaMalloc(&s->rowB, sizeof(double) * d.nxy));
+   s->row_cap = std::max(d.nxy, std::max((long long) d.nx * d.nz, (long long) d.ny * d.nz));
+   CK(cudaMalloc(&s->rowA, sizeof(double) * s->row_cap));
+   CK(cudaMalloc(&s->rowB, sizeof(double) * s->row_cap));
    CK(cudaMalloc(&s->tmp, sizeof(double) * std::max<long long>(d.nxy, std::max(d.nx, std::max(d.ny, d.nz))) * 2));
    s->obs_cap = 64;
    CK(cudaMalloc(&s->obs, sizeof(double) * s->obs_cap));
@@ -283,6 +455,7 @@ static gpe_status create_impl(const gpe_params *p, void *stream, gpe_solver *s) 
    CKS(make_coef(s, 1, d.ny, p->dy * p->dy));
    CKS(make_coef(s, 2, d.nz, p->dz * p->dz));
    CKS(make_udd(s));
+   CKS(setup_sweeps(s));
 
    // space mesh (initpsi, imag3d-mpicuda.cu:842-855)
    const long nx2 = d.nx / 2, ny2 = d.ny / 2, nz2 = d.nz / 2;
@@ -334,16 +507,6 @@ static Trap trap_of(const gpe_solver *s) {
    t.vn2 = s->p.nu * s->p.nu;
    t.vl2 = s->p.lambda * s->p.lambda;
    return t;
-}
-
-static Coef coef_of(const gpe_solver *s, int ax) {
-   Coef c;
-   c.alpha = s->alpha[ax];
-   c.gamma = s->gamma[ax];
-   c.A = s->A[ax];
-   c.A0r = s->A0r[ax];
-   c.mA = s->mA[ax];
-   return c;
 }
 
 static unsigned blocks_for(long long n, int bs) { return (unsigned) ((n + bs - 1) / bs); }
@@ -401,45 +564,50 @@ template <class R, bool CPLX> struct Impl {
       return GPE_OK;
    }
 
-   static gpe_status xsweep(gpe_solver *s, bool nu, double g, double gd) {
+   template <int AXIS, bool NU, int MSEG> static gpe_status sweep_xy_launch(gpe_solver *s, double g, double gd) {
+      auto &w = s->sw[AXIS];
       const Dims &d = s->d;
-      const long long nl = (long long) d.ny * d.nz;
-      if (nu)
-         k_xsweep<R, CPLX, true><<<blocks_for(nl, 128), 128, 0, s->st>>>((P *) s->psi, (P *) s->beta, (const R *) s->phi,
-                                                                          d, coef_of(s, 0), trap_of(s), g, gd, s->p.dt,
-                                                                          s->state);
-      else
-         k_xsweep<R, CPLX, false><<<blocks_for(nl, 128), 128, 0, s->st>>>((P *) s->psi, (P *) s->beta,
-                                                                           (const R *) s->phi, d, coef_of(s, 0),
-                                                                           trap_of(s), g, gd, s->p.dt, s->state);
+      const void *f = (const void *) k_sweep_xy<R, CPLX, AXIS, NU, MSEG>;
+      CKS(smem_attr(f, w.smem));
+      const int nzb = (d.nz + w.TW - 1) / w.TW;
+      const unsigned grid = (unsigned) ((AXIS == 0 ? d.ny : d.nx) * nzb);
+      k_sweep_xy<R, CPLX, AXIS, NU, MSEG><<<grid, w.TW * w.tab.P, w.smem, s->st>>>(
+          w.tm_psi, w.tm_phi, d, w.tab, trap_of(s), g, gd, s->p.dt, s->state, w.TW, w.boxn, w.nbox, s->err);
       CKL();
       mark(s);
       s->launches++;
       return GPE_OK;
+   }
+
+   // x sweep; with nu the pending 1/norm and calcnu are applied on load
+   // (calcnu_kernel imag3d-mpicuda.cu:1759 fused with calclux_kernel :1802).
+   static gpe_status xsweep(gpe_solver *s, bool nu, double g, double gd) {
+      if (s->sw[0].MSEG == 8) return nu ? sweep_xy_launch<0, true, 8>(s, g, gd) : sweep_xy_launch<0, false, 8>(s, g, gd);
+      return nu ? sweep_xy_launch<0, true, 16>(s, g, gd) : sweep_xy_launch<0, false, 16>(s, g, gd);
    }
 
    static gpe_status ysweep(gpe_solver *s) {
+      if (s->sw[1].MSEG == 8) return sweep_xy_launch<1, false, 8>(s, 0., 0.);
+      return sweep_xy_launch<1, false, 16>(s, 0., 0.);
+   }
+
+   template <bool SIMP, int MSEG> static gpe_status sweep_z_launch(gpe_solver *s) {
+      auto &w = s->sw[2];
       const Dims &d = s->d;
-      k_ysweep<R, CPLX><<<blocks_for((long long) d.nx * d.nz, 128), 128, 0, s->st>>>((P *) s->psi, (P *) s->beta, d,
-                                                                                   coef_of(s, 1));
+      const void *f = (const void *) k_sweep_z<R, CPLX, SIMP, MSEG>;
+      CKS(smem_attr(f, w.smem));
+      k_sweep_z<R, CPLX, SIMP, MSEG><<<blocks_for(d.nxy, w.TW), w.TW * w.tab.P, w.smem, s->st>>>(
+          (P *) s->psi, d, w.tab, w.TW, w.LS, s->wz, s->p.dz / 3., s->rowA, s->err);
       CKL();
       mark(s);
       s->launches++;
       return GPE_OK;
    }
 
+   // z sweep; with simp each row also yields its Simpson integral of |psi|^2
    static gpe_status zsweep(gpe_solver *s, bool simp) {
-      const Dims &d = s->d;
-      if (simp)
-         k_zsweep<R, CPLX, true><<<blocks_for(d.nxy, 128), 128, 0, s->st>>>((P *) s->psi, (P *) s->beta, d,
-                                                                             coef_of(s, 2), s->rowA, s->p.dz);
-      else
-         k_zsweep<R, CPLX, false><<<blocks_for(d.nxy, 128), 128, 0, s->st>>>((P *) s->psi, (P *) s->beta, d,
-                                                                              coef_of(s, 2), s->rowA, s->p.dz);
-      CKL();
-      mark(s);
-      s->launches++;
-      return GPE_OK;
+      if (s->sw[2].MSEG == 8) return simp ? sweep_z_launch<true, 8>(s) : sweep_z_launch<false, 8>(s);
+      return simp ? sweep_z_launch<true, 16>(s) : sweep_z_launch<false, 16>(s);
    }
 
    static gpe_status norm_final(gpe_solver *s, double *dev_out) {
@@ -545,6 +713,7 @@ gpe_status Impl<R, CPLX>::density(gpe_solver *s, int kind, long sx, long sy, lon
       const int first = (keep == 2) ? 1 : 2;   // z (or y for the z profile)
       const int second = (keep == 0) ? 1 : 0;  // y for x profile, x otherwise
       const int o1 = first == 0 ? 1 : 0, o2 = first == 2 ? 1 : 2;  // axes of the 2D result
+      if ((long long) n[o1] * n[o2] > s->row_cap) return fail(GPE_ERR_STATE, "row buffer too small");
       k_lineint_psi<R, CPLX><<<blocks_for((long long) n[o1] * n[o2], 128), 128, 0, s->st>>>(psi, d, first, hh[first],
                                                                                           s->rowA);
       CKL();
@@ -564,6 +733,7 @@ gpe_status Impl<R, CPLX>::density(gpe_solver *s, int kind, long sx, long sy, lon
    } else if (kind >= GPE_DEN_2D_XY && kind <= GPE_DEN_2D_YZ) {
       const int integ = 2 - (kind - GPE_DEN_2D_XY);  // xy -> z, xz -> y, yz -> x
       const int a1 = integ == 0 ? 1 : 0, a2 = integ == 2 ? 1 : 2;
+      if ((long long) n[a1] * n[a2] > s->row_cap) return fail(GPE_ERR_STATE, "row buffer too small");
       k_lineint_psi<R, CPLX><<<blocks_for((long long) n[a1] * n[a2], 128), 128, 0, s->st>>>(psi, d, integ, hh[integ],
                                                                                           s->rowA);
       CKL();
@@ -711,6 +881,19 @@ extern "C" gpe_status gpe_init_density(gpe_solver *s, const double *rho) {
 }
 
 // -------------------------------------------------------------- operators
+// Reads and clears the device status word; a bounded wait that gave up turns
+// into GPE_ERR_TIMEOUT.
+static gpe_status check_err(gpe_solver *s) {
+   uint32_t e = 0;
+   CK(cudaMemcpyAsync(&e, s->err, sizeof(e), cudaMemcpyDeviceToHost, s->st));
+   CK(cudaStreamSynchronize(s->st));
+   if (e) {
+      CK(cudaMemsetAsync(s->err, 0, sizeof(uint32_t), s->st));
+      return fail(GPE_ERR_TIMEOUT, "a bounded device wait for a bulk copy gave up");
+   }
+   return GPE_OK;
+}
+
 static gpe_status read_obs(gpe_solver *s, double *dst, int n, int off = 0) {
    CK(cudaMemcpyAsync(dst, s->obs + off, sizeof(double) * n, cudaMemcpyDeviceToHost, s->st));
    CK(cudaStreamSynchronize(s->st));
@@ -764,6 +947,7 @@ extern "C" gpe_status gpe_run(gpe_solver *s, long nsteps, double *g, double *gd,
       cudaError_t e = cudaStreamSynchronize(s->st);
       if (e != cudaSuccess) st = fail(GPE_ERR_CUDA, cudaGetErrorString(e));
    }
+   if (st == GPE_OK) st = check_err(s);
    return st;
 }
 
@@ -865,7 +1049,7 @@ extern "C" gpe_status gpe_calcluz(gpe_solver *s) {
 extern "C" gpe_status gpe_synchronize(gpe_solver *s) {
    CHECK_HANDLE(s);
    CK(cudaStreamSynchronize(s->st));
-   return GPE_OK;
+   return check_err(s);
 }
 
 extern "C" gpe_status gpe_launch_count(gpe_solver *s, long long *count) {

@@ -197,63 +197,6 @@ __global__ void k_phifix(R *__restrict__ phi, Dims d) {
 // Sweeps.
 // ===========================================================================
 
-// calcnu fused into the x sweep: psi is read once, multiplied by the pending
-// 1/norm, advanced by the nonlinear/trap exponential and then swept along x
-// (calcnu_kernel imag3d-mpicuda.cu:1759 + calclux_kernel :1802).
-template <class R, bool CPLX, bool NU>
-__global__ void __launch_bounds__(128) k_xsweep(typename Tr<R, CPLX>::P *__restrict__ psi,
-                                                typename Tr<R, CPLX>::P *__restrict__ beta,
-                                                const R *__restrict__ phi, Dims d, Coef cx, Trap trap,
-                                                double g, double gd, double dt, const State *__restrict__ st) {
-   using P = typename Tr<R, CPLX>::P;
-   const long long line = (long long) blockIdx.x * blockDim.x + threadIdx.x;
-   const long long nl = (long long) d.ny * d.nz;
-   if (line >= nl) return;
-   const int j = (int) (line / d.nz), k = (int) (line - (long long) j * d.nz);
-   const long long stx = nl;
-   const double scale = NU ? st->scale : 1.;
-   const R invN = (R) (1.0 / (double) d.npts);
-   P *ps = psi + line;
-   const R *ph = phi + line;
-   auto load = [&](int i) -> P {
-      P v = ps[(long long) i * stx];
-      if (NU) {
-         v = scl(v, scale);
-         v = nu_op<R>(v, ph[(long long) i * stx], (R) trap.v(i, j, k), (R) g, (R) gd, (R) dt, invN);
-      }
-      return v;
-   };
-   thomas_line<R, CPLX, false>(ps, beta + line, stx, d.nx, cx, load, 0.);
-}
-
-template <class R, bool CPLX>
-__global__ void __launch_bounds__(128) k_ysweep(typename Tr<R, CPLX>::P *__restrict__ psi,
-                                                typename Tr<R, CPLX>::P *__restrict__ beta, Dims d, Coef cy) {
-   using P = typename Tr<R, CPLX>::P;
-   const long long line = (long long) blockIdx.x * blockDim.x + threadIdx.x;
-   if (line >= (long long) d.nx * d.nz) return;
-   const long long i = line / d.nz, k = line - i * d.nz;
-   const long long base = i * d.ny * d.nz + k;
-   P *ps = psi + base;
-   auto load = [&](int jj) -> P { return ps[(long long) jj * d.nz]; };
-   thomas_line<R, CPLX, false>(ps, beta + base, d.nz, d.ny, cy, load, 0.);
-}
-
-// z sweep; with SIMP each row also yields its Simpson integral of |psi|^2
-// (simpint3d_kernel, diffint.cu:106) for the norm.
-template <class R, bool CPLX, bool SIMP>
-__global__ void __launch_bounds__(128) k_zsweep(typename Tr<R, CPLX>::P *__restrict__ psi,
-                                                typename Tr<R, CPLX>::P *__restrict__ beta, Dims d, Coef cz,
-                                                double *__restrict__ rowsum, double hz) {
-   using P = typename Tr<R, CPLX>::P;
-   const long long row = (long long) blockIdx.x * blockDim.x + threadIdx.x;
-   if (row >= d.nxy) return;
-   P *ps = psi + row * d.nz;
-   auto load = [&](int kk) -> P { return ps[kk]; };
-   double s = thomas_line<R, CPLX, SIMP>(ps, beta + row * d.nz, 1, d.nz, cz, load, hz);
-   if (SIMP) rowsum[row] = s;
-}
-
 // Standalone calcnu (operator-level entry point).
 template <class R, bool CPLX>
 __global__ void k_calcnu(typename Tr<R, CPLX>::P *__restrict__ psi, const R *__restrict__ phi, Dims d, Trap trap,

@@ -1,0 +1,285 @@
+// sweep_kernels.cuh -- Crank-Nicolson Thomas sweeps along x, y and z
+// (calclux/calcluy/calcluz_kernel, imag3d-mpicuda.cu:1802-1942,
+// real3d-mpicuda.cu:1902-2040) on whole lines staged in shared memory.
+//
+// A CTA owns TW lines.  The lines are brought in by one TMA tensor load (x
+// and y sweeps: box of TW z-columns by the whole line) or by one bulk copy
+// per row (z sweep), so every HBM access is a full 128-byte row segment and
+// no transpose is needed.  Each line is split into P segments of m points,
+// one thread per (line, segment); the two first-order recurrences of the
+// Thomas algorithm
+//    beta[i-1] = gamma[i] (A beta[i] - c_i),      i = n-2 .. 1
+//    psi'[i+1] = alpha[i] psi'[i] + beta[i],      i = 0 .. n-3
+// run locally from a zero carry-in, and the true values follow from the
+// carries by the exact decomposition value = local + prefix_product * carry,
+// with the prefix products of (gamma_i A) and alpha_i precomputed per axis
+// (tables M and N).  The result equals the sequential recurrence up to
+// rounding.
+#pragma once
+
+#include "kernels.cuh"
+#include "tma.cuh"
+
+namespace gpe {
+
+// Segment tables of one axis.
+struct SegTab {
+   const void *al, *ga;  // alpha[n-1], gamma[n-1]  (double or double2)
+   const void *M, *N;    // prefix products, n entries each
+   double2 A, A0r, mA;
+   int n, m, P;
+};
+
+template <class R, bool CPLX> struct SegOps {
+   using P = typename Tr<R, CPLX>::P;
+   __device__ static P ld(const void *t, int i) {
+      if constexpr (CPLX) {
+         const double2 v = ((const double2 *) t)[i];
+         return mk<R>((R) v.x, (R) v.y);
+      } else {
+         return (R) ((const double *) t)[i];
+      }
+   }
+   __device__ static P cv(double2 v) {
+      if constexpr (CPLX) return mk<R>((R) v.x, (R) v.y);
+      else return (R) v.x;
+   }
+   __device__ static P mul(P a, P b) {
+      if constexpr (CPLX) return cmul(a, b);
+      else return a * b;
+   }
+   __device__ static P fma_(P a, P b, P c) {  // a * b + c
+      if constexpr (CPLX) {
+         P r;
+         r.x = fma(a.x, b.x, c.x);
+         r.x = fma(-a.y, b.y, r.x);
+         r.y = fma(a.x, b.y, c.y);
+         r.y = fma(a.y, b.x, r.y);
+         return r;
+      } else {
+         return fma(a, b, c);
+      }
+   }
+};
+
+// Segmented Thomas sweep of line c held in shared memory at
+// s[i * es + c * cs], i in [0, n).  Called by all threads of the CTA; thread
+// (c, p) owns points [p m, min(p m + m, n) - 1].  carry is a shared scratch
+// of 2 * P * TW elements.  Writes the swept line back in place.  When simp is
+// non-null, *simp receives this thread's share of sum_i w[i] |psi'_i|^2.
+template <class R, bool CPLX, int MSEG>
+__device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, int cs, int c, int p, int TW,
+                                          const SegTab &tb, typename Tr<R, CPLX>::P *carry, const double *simp_w,
+                                          double *simp) {
+   using Op = SegOps<R, CPLX>;
+   using P = typename Tr<R, CPLX>::P;
+   const int n = tb.n, m = tb.m, NP = tb.P;
+   const int lo = p * m;
+   const bool top = (p == NP - 1);
+   const int hf = top ? n - 3 : lo + m - 1;  // last owned recurrence index
+   const int K = hf - lo + 1;                // owned points, 1 <= K <= MSEG
+   const P A = Op::cv(tb.A), A0r = Op::cv(tb.A0r), mA = Op::cv(tb.mA);
+   P *line = s + c * cs;
+   auto L = [&](int i) -> P { return line[i * es]; };
+
+   // ---- backward local recurrence: bt[q] = beta~[lo + q]
+   P bt[MSEG];
+   {
+      P b = top ? L(n - 1) : zero_of<P>();  // beta[n-2] = psi[n-1] is exact
+      // step producing beta[lo+q] uses i = lo+q+1: psi[i+1], psi[i], psi[i-1]
+      P w2 = L(lo + K + 1 <= n - 1 ? lo + K + 1 : n - 1);
+      P w1 = L(lo + K);
+#pragma unroll
+      for (int q = MSEG - 1; q >= 0; q--) {
+         if (q < K) {
+            const P w0 = L(lo + q);
+            P cc = Op::mul(mA, w2);
+            cc = cadd_any(cc, Op::mul(A0r, w1));
+            cc = csub_any(cc, Op::mul(A, w0));
+            b = Op::mul(Op::ld(tb.ga, lo + q + 1), csub_any(Op::mul(A, b), cc));
+            bt[q] = b;
+            w2 = w1;
+            w1 = w0;
+         }
+      }
+   }
+   P *cb = carry;            // [NP][TW]: beta~[lo], then beta_in
+   P *cf = carry + NP * TW;  // [NP][TW]: psi'~[hf+1], then psi'_in
+   cb[p * TW + c] = bt[0];
+   __syncthreads();  // every read of the line in this CTA is complete
+   if (p == 0) {
+      P bin = zero_of<P>();
+      for (int pp = NP - 2; pp >= 0; pp--) {
+         const int lo1 = (pp + 1) * m;
+         const P nb = Op::fma_(Op::ld(tb.M, lo1), bin, cb[(pp + 1) * TW + c]);
+         cb[(pp + 1) * TW + c] = bin;
+         bin = nb;
+      }
+      cb[c] = bin;  // beta_in of segment 0
+   }
+   __syncthreads();
+   const P bin = top ? zero_of<P>() : cb[p * TW + c];
+
+   // ---- forward local recurrence: bt[q] becomes psi'~[lo + q + 1]
+   {
+      P v = zero_of<P>();
+#pragma unroll
+      for (int q = 0; q < MSEG; q++) {
+         if (q < K) {
+            const int i = lo + q;
+            const P beta = Op::fma_(Op::ld(tb.M, i), bin, bt[q]);
+            v = Op::fma_(Op::ld(tb.al, i), v, beta);
+            bt[q] = v;
+         }
+      }
+      cf[p * TW + c] = v;  // psi'~[hf + 1]
+   }
+   __syncthreads();
+   if (p == 0) {
+      P fin = zero_of<P>();  // psi'[0] = 0
+      for (int pp = 1; pp < NP; pp++) {
+         const int lop = pp * m;
+         const P nf = Op::fma_(Op::ld(tb.N, lop), fin, cf[(pp - 1) * TW + c]);
+         cf[(pp - 1) * TW + c] = fin;
+         fin = nf;
+      }
+      cf[(NP - 1) * TW + c] = fin;
+   }
+   __syncthreads();
+   const P fin = cf[p * TW + c];
+   double acc = 0.;
+#pragma unroll
+   for (int q = 0; q < MSEG; q++) {
+      if (q < K) {
+         const int k = lo + q + 1;
+         const P v = Op::fma_(Op::ld(tb.N, k), fin, bt[q]);
+         line[k * es] = v;
+         if (simp_w) acc += simp_w[k] * (double) dens2(v);
+      }
+   }
+   if (p == 0) line[0] = zero_of<P>();
+   if (top) line[(n - 1) * es] = zero_of<P>();
+   if (simp) *simp = acc;
+}
+
+// ---------------------------------------------------------------------------
+// x or y sweep.  Tile: TW consecutive z columns of one y (x sweep) or one x
+// (y sweep) plane, the whole line along the swept axis.  With NU the x sweep
+// first applies the pending 1/norm and calcnu to the tile (needs phi).
+template <class R, bool CPLX, int AXIS, bool NU, int MSEG>
+__global__ void __launch_bounds__(256, 2) k_sweep_xy(const __grid_constant__ CUtensorMap tm_psi,
+                                                  const __grid_constant__ CUtensorMap tm_phi, Dims d, SegTab tb,
+                                                  Trap trap, double g, double gd, double dt,
+                                                  const State *__restrict__ st, int TW, int boxn, int nbox,
+                                                  uint32_t *err) {
+   using P = typename Tr<R, CPLX>::P;
+   extern __shared__ __align__(16) unsigned char smem_raw[];
+   __shared__ __align__(8) uint64_t bar;
+   const int n = tb.n;
+   const int rows = boxn * nbox;  // rows staged (>= n)
+   P *tile = (P *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);  // TMA destinations: 128-byte aligned
+   R *ptile = (R *) (tile + rows * TW);
+   P *carry = (P *) (((uintptr_t) (ptile + (NU ? rows * TW : 0)) + 15) & ~(uintptr_t) 15);
+   const int nzb = (d.nz + TW - 1) / TW;
+   const int other = blockIdx.x / nzb;  // y for the x sweep, x for the y sweep
+   const int z0 = (blockIdx.x - other * nzb) * TW;
+   constexpr int E = CPLX ? 2 : 1;
+   const uint32_t psi_bytes = (uint32_t) (rows * TW * sizeof(P));
+   const uint32_t phi_bytes = NU ? (uint32_t) (rows * TW * sizeof(R)) : 0u;
+   if (threadIdx.x == 0) {
+      mbar_init(&bar, 1);
+      fence_mbar_init();
+   }
+   __syncthreads();
+   if (threadIdx.x == 0) {
+      mbar_arrive_expect_tx(&bar, psi_bytes + phi_bytes);
+      for (int b = 0; b < nbox; b++) {
+         const int a0 = b * boxn;
+         if (AXIS == 0) tma_load_3d(tile + a0 * TW, &tm_psi, E * z0, other, a0, &bar);
+         else tma_load_3d(tile + a0 * TW, &tm_psi, E * z0, a0, other, &bar);
+         if (NU) {
+            if (AXIS == 0) tma_load_3d(ptile + a0 * TW, &tm_phi, z0, other, a0, &bar);
+            else tma_load_3d(ptile + a0 * TW, &tm_phi, z0, a0, other, &bar);
+         }
+      }
+   }
+   // a timed-out copy makes the whole CTA leave together
+   if (__syncthreads_or(!mbar_wait(&bar, 0, err))) return;
+   if (NU) {
+      const double scale = st->scale;
+      const R invN = (R) (1.0 / (double) d.npts);
+      for (int e = threadIdx.x; e < n * TW; e += blockDim.x) {
+         const int i = e / TW, cc = e - i * TW;
+         const int k = z0 + cc;
+         if (k < d.nz) {
+            const R V = (R) (AXIS == 0 ? trap.v(i, other, k) : trap.v(other, i, k));
+            tile[e] = nu_op<R>(scl(tile[e], scale), ptile[e], V, (R) g, (R) gd, (R) dt, invN);
+         }
+      }
+      __syncthreads();
+   }
+   const int c = threadIdx.x % TW, p = threadIdx.x / TW;
+   seg_sweep<R, CPLX, MSEG>(tile, TW, 1, c, p, TW, tb, carry, nullptr, nullptr);
+   fence_proxy_async();
+   __syncthreads();
+   if (threadIdx.x == 0) {
+      for (int b = 0; b < nbox; b++) {
+         const int a0 = b * boxn;
+         if (AXIS == 0) tma_store_3d(&tm_psi, E * z0, other, a0, tile + a0 * TW);
+         else tma_store_3d(&tm_psi, E * z0, a0, other, tile + a0 * TW);
+      }
+      bulk_commit();
+      bulk_wait_all();
+   }
+}
+
+// ---------------------------------------------------------------------------
+// z sweep.  Tile: TR consecutive (x, y) rows, each copied by one bulk copy to
+// a padded shared row (stride LS elements).  With SIMP every row also yields
+// its Simpson integral of |psi'|^2 (simpint over z, diffint.cu:106) for the
+// norm of the step.
+template <class R, bool CPLX, bool SIMP, int MSEG>
+__global__ void __launch_bounds__(256, 2) k_sweep_z(typename Tr<R, CPLX>::P *__restrict__ psi, Dims d, SegTab tb,
+                                                 int TR, int LS, const double *__restrict__ wz, double hz3,
+                                                 double *__restrict__ rowsum, uint32_t *err) {
+   using P = typename Tr<R, CPLX>::P;
+   extern __shared__ __align__(16) unsigned char smem_raw[];
+   __shared__ __align__(8) uint64_t bar;
+   P *tile = (P *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
+   P *carry = tile + TR * LS;
+   double *part = (double *) (carry + 2 * tb.P * TR);
+   const int nz = d.nz;
+   const long long r0 = (long long) blockIdx.x * TR;
+   const int nr = (int) ((d.nxy - r0) < TR ? (d.nxy - r0) : TR);
+   const uint32_t row_bytes = (uint32_t) (nz * sizeof(P));
+   if (threadIdx.x == 0) {
+      mbar_init(&bar, 1);
+      fence_mbar_init();
+   }
+   __syncthreads();
+   if (threadIdx.x == 0) {
+      mbar_arrive_expect_tx(&bar, row_bytes * nr);
+      for (int r = 0; r < nr; r++) bulk_load(tile + r * LS, psi + (r0 + r) * nz, row_bytes, &bar);
+   }
+   // rows beyond the grid (last tile) are zero so their sweep stays finite
+   for (int e = threadIdx.x; e < (TR - nr) * LS; e += blockDim.x) tile[nr * LS + e] = zero_of<P>();
+   if (__syncthreads_or(!mbar_wait(&bar, 0, err))) return;
+   const int c = threadIdx.x % TR, p = threadIdx.x / TR;
+   double my = 0.;
+   seg_sweep<R, CPLX, MSEG>(tile, 1, LS, c, p, TR, tb, carry, SIMP ? wz : nullptr, SIMP ? &my : nullptr);
+   if (SIMP) part[p * TR + c] = my;
+   fence_proxy_async();
+   __syncthreads();
+   if (SIMP && p == 0 && c < nr) {
+      double sum = 0.;
+      for (int pp = 0; pp < tb.P; pp++) sum += part[pp * TR + c];
+      rowsum[r0 + c] = sum * hz3;
+   }
+   if (threadIdx.x == 0) {
+      for (int r = 0; r < nr; r++) bulk_store(psi + (r0 + r) * nz, tile + r * LS, row_bytes);
+      bulk_commit();
+      bulk_wait_all();
+   }
+}
+
+}  // namespace gpe

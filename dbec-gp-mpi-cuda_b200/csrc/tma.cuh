@@ -1,0 +1,89 @@
+// tma.cuh -- Blackwell bulk-copy (TMA) and mbarrier primitives as inline PTX.
+//
+// Loads land in shared memory and complete on an mbarrier with a transaction
+// byte count; stores are bulk groups.  Every wait on an mbarrier is bounded:
+// after kMaxSpins polls the waiting thread records the failure in a global
+// status word and returns false, so a kernel never spins forever.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace gpe {
+
+constexpr uint32_t kMaxSpins = 1u << 22;
+enum : uint32_t { kErrTmaTimeout = 1u };
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t) __cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// orders this thread's generic-proxy shared-memory writes before later
+// async-proxy (bulk copy) reads of the same memory
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+   uint32_t ok;
+   asm volatile(
+       "{\n\t.reg .pred p;\n\t"
+       "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+       "selp.u32 %0, 1, 0, p;\n\t}"
+       : "=r"(ok)
+       : "r"(smem_u32(bar)), "r"(parity)
+       : "memory");
+   return ok != 0;
+}
+
+// Bounded wait for phase `parity` of `bar`.  Returns false (and sets bit
+// kErrTmaTimeout in *err) when the copy did not complete in time.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t *err) {
+   for (uint32_t i = 0; i < kMaxSpins; i++)
+      if (mbar_try_wait(bar, parity)) return true;
+   if (err) atomicOr(err, kErrTmaTimeout);
+   return false;
+}
+
+// 3D tiled tensor load global -> shared, completing on bar.
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, uint64_t *bar) {
+   asm volatile(
+       "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+       ::"r"(smem_u32(dst)), "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+       : "memory");
+}
+
+// 3D tiled tensor store shared -> global (out-of-range elements are clipped).
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap *map, int c0, int c1, int c2, const void *src) {
+   asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];"
+                ::"l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(src))
+                : "memory");
+}
+
+// Contiguous bulk copy global -> shared (16-byte aligned, size % 16 == 0).
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                : "memory");
+}
+
+// Contiguous bulk copy shared -> global.
+__device__ __forceinline__ void bulk_store(void *dst, const void *src, uint32_t bytes) {
+   asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)), "r"(bytes)
+                : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// all committed bulk stores of this thread have finished reading shared memory
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// all committed bulk stores of this thread are complete
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+}  // namespace gpe

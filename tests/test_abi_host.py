@@ -45,8 +45,8 @@ def test_invalid_parameters_rejected_without_gpu(gpe_lib, bad):
 def test_device_bytes_budget(gpe_lib):
     p = gpe_lib.make_params(1, 256, 256, 256, .2, .2, .2, 4e-4, 1., 1., 4., 25.6)
     b = gpe_lib.device_bytes(p)
-    # psi + beta (complex128) 537 MB, half spectrum 135 MB, phi 134 MB, Udd octant 17 MB
-    assert 0.80e9 < b < 0.85e9
+    # psi (complex128) 268 MB, half spectrum 135 MB, phi 134 MB, Udd octant 17 MB
+    assert 0.55e9 < b < 0.58e9
 
 
 def _cli(prog, args, cwd):
