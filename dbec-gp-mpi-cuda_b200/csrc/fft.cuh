@@ -3,27 +3,36 @@
 // src/imag3d-mpicuda/imag3d-mpicuda.cu:1460-1510; this is a project-written
 // transform, not cuFFT's).
 //
-// A CTA transforms L lines of length n held in shared memory.  Element j of
-// line l lives at base[l * ls + j * es].  Each radix-r stage (autosort
-// Stockham, decimation in time) reads from one buffer and writes the other:
-//   j in [0, n/r), k = j mod Ns,  v[t] = src[j + t n/r] * W_n^(t k n/(Ns r))
+// A CTA transforms L lines of length n held in shared memory in the
+// interleaved layout [j][L]: element j of line l at base[j * L + l].  L is
+// 128 bytes of elements (8 complex doubles, 16 complex floats), so the L
+// threads that handle one butterfly position of the L lines touch one
+// 128-byte row: bank-conflict free.  This is also the layout a TMA box of L
+// columns by the whole line lands in.
+//
+// Each radix-r stage (autosort Stockham, decimation in time) reads one
+// buffer and writes the other:
+//   j in [0, n/r), k = j mod Ns,  v[t] = src[j + t n/r] * W^(t k n/(Ns r))
 //   v = DFT_r(v),  dst[(j / Ns) Ns r + k + t Ns] = v[t],  Ns *= r
-// which leaves the result in natural order after the last stage.  The
-// twiddle table holds W_n^m = exp(-2 pi i m / n), m in [0, n), computed on
-// the host in long double; inverse transforms use conjugated twiddles and
-// are unnormalised (like cuFFT's CUFFT_INVERSE).
+// leaving the result in natural order.  W = exp(-2 pi i / n) comes from a
+// table of the n-th roots computed on the host in long double (twmul > 1
+// reads a table of a longer transform with stride twmul).  Inverse
+// transforms use conjugated twiddles and are unnormalised, like cuFFT's
+// CUFFT_INVERSE.
 #pragma once
 
 #include "common.cuh"
 
 namespace gpe {
 
-constexpr int kMaxStages = 16;
+constexpr int kMaxStages = 12;
 
 struct FftPlan {
    int n;
    int nst;
    int rad[kMaxStages];
+   int ns[kMaxStages];             // Ns before the stage
+   unsigned magic[kMaxStages];     // ceil(2^32 / Ns): j / Ns == umulhi(j, magic) for j < 2^16
 };
 
 // ---- small DFT kernels (constants are exact values of cos/sin) -------------
@@ -102,23 +111,22 @@ template <int R, class C, bool INV> __device__ __forceinline__ void dftr(C *v) {
    else dft8<C, INV>(v);
 }
 
-// One Stockham stage over L lines.  JFAST: consecutive threads take
-// consecutive j of one line (line-major layouts); otherwise consecutive
-// lines (interleaved layouts).
-template <int RAD, class C, bool INV, bool JFAST>
-__device__ __forceinline__ void fft_stage(const C *__restrict__ src, C *__restrict__ dst, int n, int L, int ls,
-                                          int es, int Ns, const C *__restrict__ tw) {
+// One Stockham stage over L interleaved lines.
+template <int RAD, int L, class C, bool INV>
+__device__ __forceinline__ void fft_stage(const C *__restrict__ src, C *__restrict__ dst, int n, int Ns,
+                                          unsigned magic, const C *__restrict__ tw, int twmul) {
    const int nr = n / RAD;
    const int nb = nr * L;
-   const int twstep = n / (Ns * RAD);
+   const int twstep = (n / (Ns * RAD)) * twmul;
    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-      int j, l;
-      if (JFAST) { j = b % nr; l = b / nr; } else { l = b % L; j = b / L; }
-      const int k = j % Ns;
+      const int l = b % L;  // L is a power of two
+      const int j = b / L;
+      const int g = Ns == 1 ? j : (int) __umulhi((unsigned) j, magic);  // j / Ns
+      const int k = j - g * Ns;
       C v[RAD];
-      const C *s = src + l * ls + j * es;
+      const C *s = src + j * L + l;
 #pragma unroll
-      for (int t = 0; t < RAD; t++) v[t] = s[t * nr * es];
+      for (int t = 0; t < RAD; t++) v[t] = s[t * nr * L];
       if (Ns > 1) {
 #pragma unroll
          for (int t = 1; t < RAD; t++) {
@@ -128,29 +136,29 @@ __device__ __forceinline__ void fft_stage(const C *__restrict__ src, C *__restri
          }
       }
       dftr<RAD, C, INV>(v);
-      C *d = dst + l * ls + ((j / Ns) * Ns * RAD + k) * es;
+      C *d = dst + (g * Ns * RAD + k) * L + l;
 #pragma unroll
-      for (int t = 0; t < RAD; t++) d[t * Ns * es] = v[t];
+      for (int t = 0; t < RAD; t++) d[t * Ns * L] = v[t];
    }
 }
 
-// Full transform; returns the buffer (a or b) that holds the result.
-// All threads of the CTA must call it; it synchronises between stages.
-template <class C, bool INV, bool JFAST>
-__device__ C *fft_lines(C *a, C *b, const FftPlan &pl, int L, int ls, int es, const C *tw) {
-   int Ns = 1;
+// Full transform of L interleaved lines; returns the buffer (a or b) holding
+// the result.  All threads of the CTA call it; it synchronises after every
+// stage.
+template <int L, class C, bool INV>
+__device__ C *fft_lines(C *a, C *b, const FftPlan &pl, const C *tw, int twmul) {
    for (int st = 0; st < pl.nst; st++) {
-      const int r = pl.rad[st];
-      switch (r) {
-      case 2: fft_stage<2, C, INV, JFAST>(a, b, pl.n, L, ls, es, Ns, tw); break;
-      case 3: fft_stage<3, C, INV, JFAST>(a, b, pl.n, L, ls, es, Ns, tw); break;
-      case 4: fft_stage<4, C, INV, JFAST>(a, b, pl.n, L, ls, es, Ns, tw); break;
-      case 5: fft_stage<5, C, INV, JFAST>(a, b, pl.n, L, ls, es, Ns, tw); break;
-      default: fft_stage<8, C, INV, JFAST>(a, b, pl.n, L, ls, es, Ns, tw); break;
+      const int Ns = pl.ns[st];
+      const unsigned mg = pl.magic[st];
+      switch (pl.rad[st]) {
+      case 2: fft_stage<2, L, C, INV>(a, b, pl.n, Ns, mg, tw, twmul); break;
+      case 3: fft_stage<3, L, C, INV>(a, b, pl.n, Ns, mg, tw, twmul); break;
+      case 4: fft_stage<4, L, C, INV>(a, b, pl.n, Ns, mg, tw, twmul); break;
+      case 5: fft_stage<5, L, C, INV>(a, b, pl.n, Ns, mg, tw, twmul); break;
+      default: fft_stage<8, L, C, INV>(a, b, pl.n, Ns, mg, tw, twmul); break;
       }
       __syncthreads();
       C *t = a; a = b; b = t;
-      Ns *= r;
    }
    return a;
 }

@@ -62,8 +62,10 @@ struct gpe_solver {
    bool cplx = false, fp32 = false;
    Dims d{};
    double par = 1.;
-   FftPlan px{}, py{}, pz{};
-   int NP = 1, LY = 1, WX = 1;
+   FftPlan px{}, py{}, ph{};  // x, y lines and half-length z lines
+   int LSr = 0, LSo = 0;                  // shared row strides of the z passes
+   CUtensorMap tm_spec_y{}, tm_spec_x{};  // spectrum tiles of the y and x passes
+   int boxy = 0, nboxy = 1, boxx = 0, nboxx = 1;
    size_t esz_psi = 8, esz_c = 16, esz_r = 8;
    void *psi = nullptr, *spec = nullptr, *phi = nullptr;
    void *twx = nullptr, *twy = nullptr, *twz = nullptr;
@@ -105,6 +107,13 @@ static bool make_plan(int n, FftPlan &pl) {
    static const int pref[] = {8, 4, 2, 3, 5};
    for (int r : pref)
       while (m % r == 0 && pl.nst < kMaxStages) { pl.rad[pl.nst++] = r; m /= r; }
+   int ns = 1;
+   for (int st = 0; st < pl.nst; st++) {
+      pl.ns[st] = ns;
+      // ceil(2^32 / ns): umulhi(j, magic) == j / ns for j, ns < 2^16; ns = 1 wraps to 0
+      pl.magic[st] = ns == 1 ? 0u : (unsigned) ((0x100000000ULL + (unsigned long long) ns - 1) / (unsigned long long) ns);
+      ns *= pl.rad[st];
+   }
    return m == 1;
 }
 
@@ -127,8 +136,8 @@ static gpe_status validate(const gpe_params *p) {
    }
    if (!(p->dx > 0 && p->dy > 0 && p->dz > 0 && p->dt > 0)) return fail(GPE_ERR_PARAM, "DX, DY, DZ, DT must be positive");
    if (!(p->cutoff > 0)) return fail(GPE_ERR_PARAM, "CUTOFF must be positive");
-   if (p->precision == GPE_PREC_MIXED && p->mode == GPE_MODE_IMAG && p->nz % 4)
-      return fail(GPE_ERR_PARAM, "mixed precision in imaginary time needs NZ divisible by 4 (16-byte rows)");
+   if (p->precision == GPE_PREC_MIXED && p->nz % 4)
+      return fail(GPE_ERR_PARAM, "mixed precision needs NZ divisible by 4 (16-byte FP32 rows)");
    return GPE_OK;
 }
 
@@ -194,19 +203,21 @@ static gpe_status make_coef(gpe_solver *s, int ax, long n, double d2) {
    s->A[ax] = make_double2(A.real(), A.imag());
    s->A0r[ax] = make_double2(A0r.real(), A0r.imag());
    s->mA[ax] = make_double2(mA.real(), mA.imag());
+   // uploaded padded to n entries (the last is 0 and never used) so that the
+   // sweep kernels can bulk-copy them in 16-byte multiples
    if (!s->cplx) {
-      std::vector<double> a(n - 1), g(n - 1);
+      std::vector<double> a(n, 0.), g(n, 0.);
       for (long i = 0; i < n - 1; i++) { a[i] = al[i].real(); g[i] = ga[i].real(); }
-      CKS(upload(&s->alpha[ax], a.data(), n - 1));
-      CKS(upload(&s->gamma[ax], g.data(), n - 1));
+      CKS(upload(&s->alpha[ax], a.data(), n));
+      CKS(upload(&s->gamma[ax], g.data(), n));
    } else {
-      std::vector<double2> a(n - 1), g(n - 1);
+      std::vector<double2> a(n, make_double2(0., 0.)), g(n, make_double2(0., 0.));
       for (long i = 0; i < n - 1; i++) {
          a[i] = make_double2(al[i].real(), al[i].imag());
          g[i] = make_double2(ga[i].real(), ga[i].imag());
       }
-      CKS(upload(&s->alpha[ax], a.data(), n - 1));
-      CKS(upload(&s->gamma[ax], g.data(), n - 1));
+      CKS(upload(&s->alpha[ax], a.data(), n));
+      CKS(upload(&s->gamma[ax], g.data(), n));
    }
    return GPE_OK;
 }
@@ -333,6 +344,7 @@ static gpe_status setup_sweeps(gpe_solver *s) {
       pick_sweep((int) nn[ax], tw_base, w.TW, w.MSEG, P);
       CKS(make_segtab(s, ax, nn[ax], h2[ax], w.MSEG, P));
       const size_t carry = 2 * (size_t) P * w.TW * esz;
+      const size_t tabs = (size_t) 4 * nn[ax] * (s->cplx ? 16 : 8);
       if (ax < 2) {
          w.boxn = (int) std::min<long>(nn[ax], 256);
          w.nbox = (int) ((nn[ax] + w.boxn - 1) / w.boxn);
@@ -340,11 +352,21 @@ static gpe_status setup_sweeps(gpe_solver *s) {
          const int by = ax == 1 ? w.boxn : 1, bx = ax == 0 ? w.boxn : 1;
          CKS(make_tmap(&w.tm_psi, s->psi, s->fp32 ? 4 : 8, E * d.nz, d.ny, d.nx, E * w.TW, by, bx));
          CKS(make_tmap(&w.tm_phi, s->phi, rsz, d.nz, d.ny, d.nx, w.TW, by, bx));
-         w.smem = 128 + rows * w.TW * esz + (ax == 0 ? rows * w.TW * rsz : 0) + 16 + carry;
+         w.smem = 128 + rows * w.TW * esz + (ax == 0 ? rows * w.TW * rsz : 0) + tabs + carry;
       } else {
          w.LS = (int) (d.nz + 16 / esz);
-         w.smem = 128 + (size_t) w.TW * w.LS * esz + carry + (size_t) P * w.TW * sizeof(double);
+         w.smem = 128 + (size_t) w.TW * w.LS * esz + tabs + carry + (size_t) P * w.TW * sizeof(double);
       }
+   }
+   // spectrum tiles: spec[x][y][kz] viewed as [nx][ny][2 nzh] scalars
+   {
+      const int L = 128 / (int) s->esz_c;
+      s->boxy = (int) std::min<long>(d.ny, 256);
+      s->nboxy = (d.ny + s->boxy - 1) / s->boxy;
+      s->boxx = (int) std::min<long>(d.nx, 256);
+      s->nboxx = (d.nx + s->boxx - 1) / s->boxx;
+      CKS(make_tmap(&s->tm_spec_y, s->spec, rsz, 2 * d.nzh, d.ny, d.nx, 2 * L, s->boxy, 1));
+      CKS(make_tmap(&s->tm_spec_x, s->spec, rsz, 2 * d.nzh, d.ny, d.nx, 2 * L, 1, s->boxx));
    }
    // Simpson weights along z: sum_k wz[k] f[k] * dz / 3 equals simpint (diffint.cu:37-66)
    std::vector<double> wz(d.nz, 0.);
@@ -360,8 +382,9 @@ static gpe_status setup_sweeps(gpe_solver *s) {
 }
 
 // initpotdd (imag3d-mpicuda.cu:945-980) on the octant |kx| <= nx/2,
-// |ky| <= ny/2, kz <= nz/2: Udd depends on kx^2, ky^2, kz^2 only, and the
-// squares of the reference's negative k values equal those of the octant.
+// |ky| <= ny/2, kz <= nz/2, stored [|kx|][|ky|][kz]: Udd depends on kx^2,
+// ky^2, kz^2 only, and the squares of the reference's negative k values equal
+// those of the octant.
 static gpe_status make_udd(gpe_solver *s) {
    const long nx = s->p.nx, ny = s->p.ny, nz = s->p.nz;
    const long nxh = nx / 2 + 1, nyh = ny / 2 + 1, nzh = nz / 2 + 1;
@@ -372,13 +395,13 @@ static gpe_status make_udd(gpe_solver *s) {
    for (long i = 0; i < nyh; i++) { double k = i * dky; ky2[i] = k * k; }
    for (long i = 0; i < nzh; i++) { double k = i * dkz; kz2[i] = k * k; }
    std::vector<double> u((size_t) (nzh * nxh * nyh));
-   for (long k = 0; k < nzh; k++)
-      for (long i = 0; i < nxh; i++)
-         for (long j = 0; j < nyh; j++) {
+   for (long i = 0; i < nxh; i++)
+      for (long j = 0; j < nyh; j++)
+         for (long k = 0; k < nzh; k++) {
             const double xk = std::sqrt(kz2[k] + kx2[i] + ky2[j]);
             const double tmp = 1. + 3. * std::cos(xk * cutoff) / (xk * xk * cutoff * cutoff) -
                                3. * std::sin(xk * cutoff) / (xk * xk * xk * cutoff * cutoff * cutoff);
-            u[(size_t) ((k * nxh + i) * nyh + j)] = (4. * pi * (3. * kz2[k] / (kx2[i] + ky2[j] + kz2[k]) - 1.) / 3.) * tmp;
+            u[(size_t) ((i * nyh + j) * nzh + k)] = (4. * pi * (3. * kz2[k] / (kx2[i] + ky2[j] + kz2[k]) - 1.) / 3.) * tmp;
          }
    u[0] = 0.;  // imag3d-mpicuda.cu:975-977
    void *dp = nullptr;
@@ -422,16 +445,13 @@ static gpe_status create_impl(const gpe_params *p, void *stream, gpe_solver *s) 
    d.npts = d.nxy * d.nz;
    make_plan(d.nx, s->px);
    make_plan(d.ny, s->py);
-   make_plan(d.nz, s->pz);
+   make_plan(d.nz / 2, s->ph);
    const size_t r = s->fp32 ? 4 : 8;
    s->esz_r = r;
    s->esz_c = 2 * r;
    s->esz_psi = psi_esz(p);
-   // tile sizes: ~64 KB of ping-pong shared memory per CTA
-   const long long budget = 64 * 1024;
-   s->NP = std::min(32, floor_pow2(std::max(1LL, budget / (long long) (2 * (d.nz + 2) * s->esz_c))));
-   s->LY = std::min(32, floor_pow2(std::max(1LL, budget / (long long) (2 * d.ny * s->esz_c))));
-   s->WX = std::max(4, std::min(16, floor_pow2(std::max(1LL, budget / (long long) (2 * d.nx * s->esz_c)))));
+   s->LSr = (int) (d.nz + 16 / s->esz_psi);
+   s->LSo = (int) (d.nz + 16 / s->esz_r);
 
    CK(cudaMalloc(&s->psi, s->esz_psi * d.npts));
    CK(cudaMalloc(&s->spec, s->esz_c * (size_t) d.nzh * d.nxy));
@@ -522,38 +542,42 @@ template <class R, bool CPLX> struct Impl {
 
    static gpe_status psidd2(gpe_solver *s) {
       const Dims &d = s->d;
+      constexpr int L = FftL<R>::L;
+      const int h = d.nz / 2;
       C *spec = (C *) s->spec;
+      const unsigned grows = blocks_for(d.nxy, L);
       {
-         const size_t sm = (size_t) (2 * s->NP * (d.nz + 2) + d.nz) * sizeof(C);
+         const size_t sm = 128 + (size_t) L * s->LSr * sizeof(P) + 2 * (size_t) h * L * sizeof(C) + d.nz * sizeof(C);
          CKS(smem_attr((const void *) k_zfwd<R, CPLX>, sm));
-         k_zfwd<R, CPLX><<<blocks_for(d.nxy, 2 * s->NP), 256, sm, s->st>>>((const P *) s->psi, spec, d, s->pz,
-                                                                            (const C *) s->twz, s->NP);
+         k_zfwd<R, CPLX><<<grows, 256, sm, s->st>>>((const P *) s->psi, spec, d, s->ph, (const C *) s->twz, s->LSr, s->err);
          CKL();
          mark(s);
       }
-      const size_t smy = (size_t) (2 * s->LY * d.ny + d.ny) * sizeof(C);
-      const unsigned gy = blocks_for((long long) d.nzh * d.nx, s->LY);
+      const int nkb = (d.nzh + L - 1) / L;
+      const size_t smy = 128 + 2 * (size_t) s->boxy * s->nboxy * L * sizeof(C) + d.ny * sizeof(C);
       CKS(smem_attr((const void *) k_yfft<R, false>, smy));
-      k_yfft<R, false><<<gy, 256, smy, s->st>>>(spec, d, s->py, (const C *) s->twy, s->LY);
+      k_yfft<R, false><<<(unsigned) (d.nx * nkb), 256, smy, s->st>>>(s->tm_spec_y, d, s->py, (const C *) s->twy, s->boxy,
+                                                                     s->nboxy, s->err);
       CKL();
       mark(s);
       {
-         const size_t sm = (size_t) (2 * d.nx * s->WX + d.nx) * sizeof(C);
-         const unsigned gx = (unsigned) (d.nzh * ((d.ny + s->WX - 1) / s->WX));
+         const size_t sm = 128 + 2 * (size_t) s->boxx * s->nboxx * L * sizeof(C) + d.nx * sizeof(C);
          CKS(smem_attr((const void *) k_xconv<R>, sm));
-         k_xconv<R><<<gx, 256, sm, s->st>>>(spec, d, s->px, (const C *) s->twx, s->udd, s->state, s->WX);
+         k_xconv<R><<<(unsigned) (d.ny * nkb), 256, sm, s->st>>>(s->tm_spec_x, d, s->px, (const C *) s->twx, s->udd,
+                                                                 s->state, s->boxx, s->nboxx, s->err);
          CKL();
          mark(s);
       }
       CKS(smem_attr((const void *) k_yfft<R, true>, smy));
-      k_yfft<R, true><<<gy, 256, smy, s->st>>>(spec, d, s->py, (const C *) s->twy, s->LY);
+      k_yfft<R, true><<<(unsigned) (d.nx * nkb), 256, smy, s->st>>>(s->tm_spec_y, d, s->py, (const C *) s->twy, s->boxy,
+                                                                    s->nboxy, s->err);
       CKL();
       mark(s);
       {
-         const size_t sm = (size_t) (2 * s->NP * (d.nz + 2) + d.nz) * sizeof(C);
+         const size_t in_el = std::max((size_t) L * d.nzh, ((size_t) L * s->LSo * sizeof(R) + sizeof(C) - 1) / sizeof(C));
+         const size_t sm = 128 + ((in_el + 7) & ~(size_t) 7) * sizeof(C) + 2 * (size_t) h * L * sizeof(C) + d.nz * sizeof(C);
          CKS(smem_attr((const void *) k_zinv<R>, sm));
-         k_zinv<R><<<blocks_for(d.nxy, 2 * s->NP), 256, sm, s->st>>>(spec, (R *) s->phi, d, s->pz, (const C *) s->twz,
-                                                                      s->NP);
+         k_zinv<R><<<grows, 256, sm, s->st>>>(spec, (R *) s->phi, d, s->ph, (const C *) s->twz, s->LSo, s->err);
          CKL();
          mark(s);
       }

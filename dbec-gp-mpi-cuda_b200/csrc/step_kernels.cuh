@@ -3,169 +3,222 @@
 #pragma once
 
 #include "kernels.cuh"
+#include "tma.cuh"
 
 namespace gpe {
 
 // ===========================================================================
 // Dipolar convolution phi = IFFT[Udd * FFT[|psi|^2]] (calcpsidd2_mem,
-// imag3d-mpicuda.cu:1460-1510) as five FFT passes over the half spectrum.
+// imag3d-mpicuda.cu:1460-1510) as four FFT passes over the half spectrum
+// spec[x][y][kz], kz in [0, nz/2], plus the boundary planes.
+//
+// z passes: each real row of length nz is transformed as a complex line of
+// length h = nz/2 (z[m] = x[2m] + i x[2m+1]) and split/merged with
+//   X[k] = E + W^k O,  E = (Z_k + conj Z_{h-k})/2,  O = (Z_k - conj Z_{h-k})/(2i)
+// (forward) and Z_k = (X_k + conj X_{h-k}) + i (X_k - conj X_{h-k}) W^-k
+// (inverse), W = exp(-2 pi i / nz).  Rows arrive and leave by bulk copies.
+// y and x passes: a TMA box of L kz columns by the whole line lands in the
+// interleaved layout the FFT engine works in.
 // ===========================================================================
 
-// Pass 1: |psi|^2 rows -> half spectrum along z.  Two real rows form one
-// complex line (x_a + i x_b); after the FFT the two half spectra are split
-// with X_a = (Z_k + conj Z_{n-k})/2, X_b = (Z_k - conj Z_{n-k})/(2i).
+template <class R> struct FftL { static constexpr int L = 128 / (2 * (int) sizeof(R)); };
+
+// Pass 1: |psi|^2 rows -> half spectrum rows (L rows per CTA).
 template <class R, bool CPLX>
 __global__ void __launch_bounds__(256) k_zfwd(const typename Tr<R, CPLX>::P *__restrict__ psi,
-                                              cpx<R> *__restrict__ spec, Dims d, FftPlan pz,
-                                              const cpx<R> *__restrict__ twz, int NP) {
+                                              cpx<R> *__restrict__ spec, Dims d, FftPlan ph,
+                                              const cpx<R> *__restrict__ twz, int LSr, uint32_t *err) {
    using C = cpx<R>;
+   using P = typename Tr<R, CPLX>::P;
+   constexpr int L = FftL<R>::L;
    extern __shared__ __align__(16) unsigned char smem_raw[];
-   const int nz = d.nz, ls = nz + 2;
-   C *bufA = (C *) smem_raw;
-   C *bufB = bufA + NP * ls;
-   C *tw = bufB + NP * ls;
-   for (int i = threadIdx.x; i < nz; i += blockDim.x) tw[i] = twz[i];
-   const long long r0 = (long long) blockIdx.x * (2 * NP);
-   for (int e = threadIdx.x; e < 2 * NP * nz; e += blockDim.x) {
-      const int rr = e / nz, k = e - rr * nz;
-      const long long row = r0 + rr;
-      R v = (R) 0;
-      if (row < d.nxy) v = dens2(psi[row * nz + k]);
-      C *slot = &bufA[(rr >> 1) * ls + k];
-      if (rr & 1) slot->y = v; else slot->x = v;
+   __shared__ __align__(8) uint64_t bar;
+   const int nz = d.nz, h = nz / 2, nzh = d.nzh;
+   // layout: rows [L][LSr] (later the output rows [L][nzh]) | bufA | bufB | twiddles
+   P *rows = (P *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
+   C *bufA = (C *) (rows + L * LSr);
+   C *bufB = bufA + h * L;
+   C *tw = bufB + h * L;
+   const long long r0 = (long long) blockIdx.x * L;
+   const int nr = (int) ((d.nxy - r0) < L ? (d.nxy - r0) : L);
+   const uint32_t row_bytes = (uint32_t) (nz * sizeof(P));
+   if (threadIdx.x == 0) {
+      mbar_init(&bar, 1);
+      fence_mbar_init();
    }
    __syncthreads();
-   C *res = fft_lines<C, false, true>(bufA, bufB, pz, NP, ls, 1, tw);
-   const int nzh = d.nzh;
-   for (int e = threadIdx.x; e < 2 * NP * nzh; e += blockDim.x) {
-      const int k = e / (2 * NP), rr = e - k * (2 * NP);
-      const long long row = r0 + rr;
-      if (row >= d.nxy) continue;
-      const C *line = res + (rr >> 1) * ls;
-      C Z = line[k];
-      C Zc = cconj(line[k == 0 ? 0 : nz - k]);
-      C X;
-      if (rr & 1) {
-         C t = csub(Z, Zc);
-         X = mk<R>(t.y * (R) 0.5, -t.x * (R) 0.5);
-      } else {
-         C t = cadd(Z, Zc);
-         X = mk<R>(t.x * (R) 0.5, t.y * (R) 0.5);
-      }
-      spec[(long long) k * d.nxy + row] = X;
+   if (threadIdx.x == 0) {
+      mbar_arrive_expect_tx(&bar, row_bytes * nr + (uint32_t) (nz * sizeof(C)));
+      bulk_load(tw, twz, (uint32_t) (nz * sizeof(C)), &bar);
+      for (int r = 0; r < nr; r++) bulk_load(rows + r * LSr, psi + (r0 + r) * nz, row_bytes, &bar);
+   }
+   for (int e = threadIdx.x; e < (L - nr) * LSr; e += blockDim.x) rows[nr * LSr + e] = zero_of<P>();
+   if (__syncthreads_or(!mbar_wait(&bar, 0, err))) return;
+   for (int e = threadIdx.x; e < h * L; e += blockDim.x) {
+      const int l = e % L, m = e / L;
+      const P *rw = rows + l * LSr + 2 * m;
+      bufA[e] = mk<R>(dens2(rw[0]), dens2(rw[1]));
+   }
+   __syncthreads();
+   const C *Z = fft_lines<L, C, false>(bufA, bufB, ph, tw, 2);
+   C *out = (C *) rows;  // [L][nzh]; the rows are no longer read
+   for (int e = threadIdx.x; e < nzh * L; e += blockDim.x) {
+      const int l = e % L, k = e / L;
+      const C a = Z[(k == h ? 0 : k) * L + l];
+      const C b = cconj(Z[(k == 0 ? 0 : h - k) * L + l]);
+      const C E = cscale(cadd(a, b), (R) 0.5);
+      const C t = csub(a, b);
+      const C O = mk<R>(t.y * (R) 0.5, -t.x * (R) 0.5);
+      out[l * nzh + k] = cadd(E, cmul(tw[k], O));
+   }
+   fence_proxy_async();
+   __syncthreads();
+   if (threadIdx.x == 0) {
+      bulk_store(spec + r0 * nzh, out, (uint32_t) (nr * nzh * sizeof(C)));
+      bulk_commit();
+      bulk_wait_all();
    }
 }
 
-// Passes 2 and 4: FFT along y; lines are contiguous (spec[(k nx + x) ny + y]).
+// Passes 2 and 4: FFT along y of L kz columns of one x plane.
 template <class R, bool INV>
-__global__ void __launch_bounds__(256) k_yfft(cpx<R> *__restrict__ spec, Dims d, FftPlan py,
-                                              const cpx<R> *__restrict__ twy, int LY) {
+__global__ void __launch_bounds__(256) k_yfft(const __grid_constant__ CUtensorMap tm, Dims d, FftPlan py,
+                                              const cpx<R> *__restrict__ twy, int boxn, int nbox, uint32_t *err) {
    using C = cpx<R>;
+   constexpr int L = FftL<R>::L;
    extern __shared__ __align__(16) unsigned char smem_raw[];
-   const int ny = d.ny;
-   C *bufA = (C *) smem_raw;
-   C *bufB = bufA + LY * ny;
-   C *tw = bufB + LY * ny;
-   for (int i = threadIdx.x; i < ny; i += blockDim.x) tw[i] = twy[i];
-   const long long nlines = (long long) d.nzh * d.nx;
-   const long long l0 = (long long) blockIdx.x * LY;
-   const int nl = (int) ((nlines - l0) < LY ? (nlines - l0) : LY);
-   const C *src = spec + l0 * ny;
-   for (int e = threadIdx.x; e < nl * ny; e += blockDim.x) bufA[e] = src[e];
-   for (int e = nl * ny + threadIdx.x; e < LY * ny; e += blockDim.x) bufA[e] = mk<R>(0, 0);
-   __syncthreads();
-   C *res = fft_lines<C, INV, true>(bufA, bufB, py, LY, ny, 1, tw);
-   C *dst = spec + l0 * ny;
-   for (int e = threadIdx.x; e < nl * ny; e += blockDim.x) dst[e] = res[e];
-}
-
-// Pass 3: FFT along x, multiply by Udd(k) * scale^2, inverse FFT along x.
-// A CTA takes W consecutive y columns of one kz plane (interleaved layout:
-// element (column c, x) at x * W + c).
-template <class R>
-__global__ void __launch_bounds__(256) k_xconv(cpx<R> *__restrict__ spec, Dims d, FftPlan px,
-                                               const cpx<R> *__restrict__ twx, const double *__restrict__ udd,
-                                               const State *__restrict__ st, int W) {
-   using C = cpx<R>;
-   extern __shared__ __align__(16) unsigned char smem_raw[];
-   const int nx = d.nx, ny = d.ny;
-   C *bufA = (C *) smem_raw;
-   C *bufB = bufA + nx * W;
-   C *tw = bufB + nx * W;
-   for (int i = threadIdx.x; i < nx; i += blockDim.x) tw[i] = twx[i];
-   const int nyb = (ny + W - 1) / W;
-   const int kz = blockIdx.x / nyb;
-   const int y0 = (blockIdx.x - kz * nyb) * W;
-   C *plane = spec + (long long) kz * d.nxy;
-   for (int e = threadIdx.x; e < nx * W; e += blockDim.x) {
-      const int x = e / W, c = e - x * W;
-      const int y = y0 + c;
-      bufA[e] = (y < ny) ? plane[(long long) x * ny + y] : mk<R>(0, 0);
+   __shared__ __align__(8) uint64_t bar;
+   const int ny = d.ny, rows = boxn * nbox;
+   C *bufA = (C *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
+   C *bufB = bufA + rows * L;
+   C *tw = bufB + rows * L;
+   const int nkb = (d.nzh + L - 1) / L;
+   const int x = blockIdx.x / nkb, k0 = (blockIdx.x - x * nkb) * L;
+   if (threadIdx.x == 0) {
+      mbar_init(&bar, 1);
+      fence_mbar_init();
    }
    __syncthreads();
-   C *res = fft_lines<C, false, false>(bufA, bufB, px, W, 1, W, tw);
+   if (threadIdx.x == 0) {
+      mbar_arrive_expect_tx(&bar, (uint32_t) (rows * L * sizeof(C) + ny * sizeof(C)));
+      bulk_load(tw, twy, (uint32_t) (ny * sizeof(C)), &bar);
+      for (int b = 0; b < nbox; b++) tma_load_3d(bufA + b * boxn * L, &tm, 2 * k0, b * boxn, x, &bar);
+   }
+   if (__syncthreads_or(!mbar_wait(&bar, 0, err))) return;
+   C *res = fft_lines<L, C, INV>(bufA, bufB, py, tw, 1);
+   fence_proxy_async();
+   __syncthreads();
+   if (threadIdx.x == 0) {
+      for (int b = 0; b < nbox; b++) tma_store_3d(&tm, 2 * k0, b * boxn, x, res + b * boxn * L);
+      bulk_commit();
+      bulk_wait_all();
+   }
+}
+
+// Pass 3: FFT along x, multiply by Udd(k) * scale^2, inverse FFT along x, for
+// L kz columns of one y plane.  Udd octant layout [|kx|][|ky|][kz].
+template <class R>
+__global__ void __launch_bounds__(256) k_xconv(const __grid_constant__ CUtensorMap tm, Dims d, FftPlan px,
+                                               const cpx<R> *__restrict__ twx, const double *__restrict__ udd,
+                                               const State *__restrict__ st, int boxn, int nbox, uint32_t *err) {
+   using C = cpx<R>;
+   constexpr int L = FftL<R>::L;
+   extern __shared__ __align__(16) unsigned char smem_raw[];
+   __shared__ __align__(8) uint64_t bar;
+   const int nx = d.nx, ny = d.ny, rows = boxn * nbox;
+   C *bufA = (C *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
+   C *bufB = bufA + rows * L;
+   C *tw = bufB + rows * L;
+   const int nkb = (d.nzh + L - 1) / L;
+   const int y = blockIdx.x / nkb, k0 = (blockIdx.x - y * nkb) * L;
+   if (threadIdx.x == 0) {
+      mbar_init(&bar, 1);
+      fence_mbar_init();
+   }
+   __syncthreads();
+   if (threadIdx.x == 0) {
+      mbar_arrive_expect_tx(&bar, (uint32_t) (rows * L * sizeof(C) + nx * sizeof(C)));
+      bulk_load(tw, twx, (uint32_t) (nx * sizeof(C)), &bar);
+      for (int b = 0; b < nbox; b++) tma_load_3d(bufA + b * boxn * L, &tm, 2 * k0, y, b * boxn, &bar);
+   }
+   if (__syncthreads_or(!mbar_wait(&bar, 0, err))) return;
+   C *res = fft_lines<L, C, false>(bufA, bufB, px, tw, 1);
    C *oth = (res == bufA) ? bufB : bufA;
    const double s2 = st->scale2;
-   const int nxh = nx / 2 + 1, nyh = ny / 2 + 1;
-   const double *uplane = udd + (long long) kz * nxh * nyh;
-   for (int e = threadIdx.x; e < nx * W; e += blockDim.x) {
-      const int x = e / W, c = e - x * W;
-      int y = y0 + c;
-      if (y >= ny) y = ny - 1;
-      const int ax = (x <= nx / 2) ? x : nx - x;
-      const int ay = (y <= ny / 2) ? y : ny - y;
-      const R u = (R) (uplane[ax * nyh + ay] * s2);
+   const int nyh = ny / 2 + 1, nzh = d.nzh;
+   const int ay = (y <= ny / 2) ? y : ny - y;
+   for (int e = threadIdx.x; e < nx * L; e += blockDim.x) {
+      const int xx = e / L, c = e - xx * L;
+      const int k = k0 + c < nzh ? k0 + c : nzh - 1;
+      const int ax = (xx <= nx / 2) ? xx : nx - xx;
+      const R u = (R) (udd[((long long) ax * nyh + ay) * nzh + k] * s2);
       res[e] = cscale(res[e], u);
    }
    __syncthreads();
-   C *fin = fft_lines<C, true, false>(res, oth, px, W, 1, W, tw);
-   for (int e = threadIdx.x; e < nx * W; e += blockDim.x) {
-      const int x = e / W, c = e - x * W;
-      const int y = y0 + c;
-      if (y < ny) plane[(long long) x * ny + y] = fin[e];
+   C *fin = fft_lines<L, C, true>(res, oth, px, tw, 1);
+   fence_proxy_async();
+   __syncthreads();
+   if (threadIdx.x == 0) {
+      for (int b = 0; b < nbox; b++) tma_store_3d(&tm, 2 * k0, y, b * boxn, fin + b * boxn * L);
+      bulk_commit();
+      bulk_wait_all();
    }
 }
 
-// Pass 5: Hermitian inverse along z -> phi rows (two rows per complex line).
+// Pass 5: half spectrum rows -> phi rows (unnormalised inverse, Hermitian).
 template <class R>
 __global__ void __launch_bounds__(256) k_zinv(const cpx<R> *__restrict__ spec, R *__restrict__ phi, Dims d,
-                                              FftPlan pz, const cpx<R> *__restrict__ twz, int NP) {
+                                              FftPlan ph, const cpx<R> *__restrict__ twz, int LSo, uint32_t *err) {
    using C = cpx<R>;
+   constexpr int L = FftL<R>::L;
    extern __shared__ __align__(16) unsigned char smem_raw[];
-   const int nz = d.nz, nzh = d.nzh, ls = nz + 2;
-   C *bufA = (C *) smem_raw;
-   C *bufB = bufA + NP * ls;
-   C *tw = bufB + NP * ls;
-   for (int i = threadIdx.x; i < nz; i += blockDim.x) tw[i] = twz[i];
-   const long long r0 = (long long) blockIdx.x * (2 * NP);
-   C *half = bufB;  // [2NP][nzh]
-   for (int e = threadIdx.x; e < 2 * NP * nzh; e += blockDim.x) {
-      const int k = e / (2 * NP), rr = e - k * (2 * NP);
-      const long long row = r0 + rr;
-      half[rr * nzh + k] = (row < d.nxy) ? spec[(long long) k * d.nxy + row] : mk<R>(0, 0);
+   __shared__ __align__(8) uint64_t bar;
+   const int nz = d.nz, h = nz / 2, nzh = d.nzh;
+   // layout: input rows [L][nzh] (later the phi rows [L][LSo]) | bufA | bufB | twiddles
+   C *in = (C *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
+   const int in_elems = ((L * nzh) > (L * LSo + 1) / 2 ? (L * nzh) : (L * LSo + 1) / 2);
+   C *bufA = in + ((in_elems + 7) & ~7);
+   C *bufB = bufA + h * L;
+   C *tw = bufB + h * L;
+   const long long r0 = (long long) blockIdx.x * L;
+   const int nr = (int) ((d.nxy - r0) < L ? (d.nxy - r0) : L);
+   if (threadIdx.x == 0) {
+      mbar_init(&bar, 1);
+      fence_mbar_init();
    }
    __syncthreads();
-   for (int e = threadIdx.x; e < NP * nz; e += blockDim.x) {
-      const int p = e / nz, k = e - p * nz;
-      C a, b;
-      if (k < nzh) {
-         a = half[(2 * p) * nzh + k];
-         b = half[(2 * p + 1) * nzh + k];
-      } else {
-         a = cconj(half[(2 * p) * nzh + nz - k]);
-         b = cconj(half[(2 * p + 1) * nzh + nz - k]);
-      }
-      if (k == 0 || 2 * k == nz) { a.y = 0; b.y = 0; }
-      bufA[p * ls + k] = mk<R>(a.x - b.y, a.y + b.x);
+   if (threadIdx.x == 0) {
+      mbar_arrive_expect_tx(&bar, (uint32_t) (nr * nzh * sizeof(C) + nz * sizeof(C)));
+      bulk_load(tw, twz, (uint32_t) (nz * sizeof(C)), &bar);
+      bulk_load(in, spec + r0 * nzh, (uint32_t) (nr * nzh * sizeof(C)), &bar);
+   }
+   for (int e = threadIdx.x; e < (L - nr) * nzh; e += blockDim.x) in[nr * nzh + e] = mk<R>(0, 0);
+   if (__syncthreads_or(!mbar_wait(&bar, 0, err))) return;
+   for (int e = threadIdx.x; e < h * L; e += blockDim.x) {
+      const int l = e % L, k = e / L;
+      C a = in[l * nzh + k];
+      C b = in[l * nzh + h - k];
+      if (k == 0) { a.y = 0; b.y = 0; }  // DC and Nyquist bins are real
+      b = cconj(b);
+      const C E = cadd(a, b);
+      const C O = cmul(csub(a, b), cconj(tw[k]));
+      bufA[e] = mk<R>(E.x - O.y, E.y + O.x);
    }
    __syncthreads();
-   C *res = fft_lines<C, true, true>(bufA, bufB, pz, NP, ls, 1, tw);
-   for (int e = threadIdx.x; e < 2 * NP * nz; e += blockDim.x) {
-      const int rr = e / nz, k = e - rr * nz;
-      const long long row = r0 + rr;
-      if (row >= d.nxy) continue;
-      const C v = res[(rr >> 1) * ls + k];
-      phi[row * nz + k] = (rr & 1) ? v.y : v.x;
+   const C *z = fft_lines<L, C, true>(bufA, bufB, ph, tw, 2);
+   R *out = (R *) in;  // [L][LSo]
+   for (int e = threadIdx.x; e < h * L; e += blockDim.x) {
+      const int l = e % L, m = e / L;
+      const C v = z[e];
+      out[l * LSo + 2 * m] = v.x;
+      out[l * LSo + 2 * m + 1] = v.y;
+   }
+   fence_proxy_async();
+   __syncthreads();
+   if (threadIdx.x == 0) {
+      for (int r = 0; r < nr; r++) bulk_store(phi + (r0 + r) * nz, out + r * LSo, (uint32_t) (nz * sizeof(R)));
+      bulk_commit();
+      bulk_wait_all();
    }
 }
 

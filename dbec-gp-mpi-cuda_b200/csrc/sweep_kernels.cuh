@@ -24,7 +24,7 @@ namespace gpe {
 
 // Segment tables of one axis.
 struct SegTab {
-   const void *al, *ga;  // alpha[n-1], gamma[n-1]  (double or double2)
+   const void *al, *ga;  // alpha, gamma padded to n entries (double or double2)
    const void *M, *N;    // prefix products, n entries each
    double2 A, A0r, mA;
    int n, m, P;
@@ -64,16 +64,28 @@ template <class R, bool CPLX> struct SegOps {
 
 // Segmented Thomas sweep of line c held in shared memory at
 // s[i * es + c * cs], i in [0, n).  Called by all threads of the CTA; thread
-// (c, p) owns points [p m, min(p m + m, n) - 1].  carry is a shared scratch
-// of 2 * P * TW elements.  Writes the swept line back in place.  When simp is
-// non-null, *simp receives this thread's share of sum_i w[i] |psi'_i|^2.
+// (c, p) owns recurrence indices [p m, hf].  tabs points to the axis tables
+// staged in shared memory: alpha, gamma, M, N, n entries each.  ca and cb are
+// shared scratch of P * TW elements each.  Writes the swept line back in
+// place.  When simp_w is non-null, *simp receives this thread's share of
+// sum_i simp_w[i] |psi'_i|^2.
+//
+// Carries: segment p maps the value entering at its top (index hf+1) to the
+// value at its bottom (index lo) by the affine map x -> b + a x with
+// a = M[lo], b = beta~[lo]; the value entering segment p is the composition
+// of the maps of all segments above it (a suffix scan, Kogge-Stone in log2 P
+// rounds).  The forward recurrence composes x -> psi'~[hf+1] + N[hf+1] x from
+// the bottom (a prefix scan).
 template <class R, bool CPLX, int MSEG>
 __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, int cs, int c, int p, int TW,
-                                          const SegTab &tb, typename Tr<R, CPLX>::P *carry, const double *simp_w,
-                                          double *simp) {
+                                          const SegTab &tb, const unsigned char *tabs,
+                                          typename Tr<R, CPLX>::P *ca, typename Tr<R, CPLX>::P *cb,
+                                          const double *simp_w, double *simp) {
    using Op = SegOps<R, CPLX>;
    using P = typename Tr<R, CPLX>::P;
+   constexpr int TE = CPLX ? 16 : 8;  // bytes of one table entry (double or double2)
    const int n = tb.n, m = tb.m, NP = tb.P;
+   const void *t_al = tabs, *t_ga = tabs + n * TE, *t_M = tabs + 2 * n * TE, *t_N = tabs + 3 * n * TE;
    const int lo = p * m;
    const bool top = (p == NP - 1);
    const int hf = top ? n - 3 : lo + m - 1;  // last owned recurrence index
@@ -81,13 +93,14 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
    const P A = Op::cv(tb.A), A0r = Op::cv(tb.A0r), mA = Op::cv(tb.mA);
    P *line = s + c * cs;
    auto L = [&](int i) -> P { return line[i * es]; };
+   const int me = p * TW + c;
 
    // ---- backward local recurrence: bt[q] = beta~[lo + q]
    P bt[MSEG];
    {
       P b = top ? L(n - 1) : zero_of<P>();  // beta[n-2] = psi[n-1] is exact
-      // step producing beta[lo+q] uses i = lo+q+1: psi[i+1], psi[i], psi[i-1]
-      P w2 = L(lo + K + 1 <= n - 1 ? lo + K + 1 : n - 1);
+      // the step producing beta[lo+q] uses i = lo+q+1: psi[i+1], psi[i], psi[i-1]
+      P w2 = L(lo + K + 1);
       P w1 = L(lo + K);
 #pragma unroll
       for (int q = MSEG - 1; q >= 0; q--) {
@@ -96,70 +109,87 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
             P cc = Op::mul(mA, w2);
             cc = cadd_any(cc, Op::mul(A0r, w1));
             cc = csub_any(cc, Op::mul(A, w0));
-            b = Op::mul(Op::ld(tb.ga, lo + q + 1), csub_any(Op::mul(A, b), cc));
+            b = Op::mul(Op::ld(t_ga, lo + q + 1), csub_any(Op::mul(A, b), cc));
             bt[q] = b;
             w2 = w1;
             w1 = w0;
          }
       }
    }
-   P *cb = carry;            // [NP][TW]: beta~[lo], then beta_in
-   P *cf = carry + NP * TW;  // [NP][TW]: psi'~[hf+1], then psi'_in
-   cb[p * TW + c] = bt[0];
-   __syncthreads();  // every read of the line in this CTA is complete
-   if (p == 0) {
-      P bin = zero_of<P>();
-      for (int pp = NP - 2; pp >= 0; pp--) {
-         const int lo1 = (pp + 1) * m;
-         const P nb = Op::fma_(Op::ld(tb.M, lo1), bin, cb[(pp + 1) * TW + c]);
-         cb[(pp + 1) * TW + c] = bin;
-         bin = nb;
+   // ---- suffix scan of the backward maps
+   P sa = top ? zero_of<P>() : Op::ld(t_M, lo), sb = bt[0];
+   for (int dd = 1; dd < NP; dd <<= 1) {
+      ca[me] = sa;
+      cb[me] = sb;
+      __syncthreads();
+      if (p + dd < NP) {
+         const P a2 = ca[me + dd * TW], b2 = cb[me + dd * TW];
+         sb = Op::fma_(sa, b2, sb);
+         sa = Op::mul(sa, a2);
       }
-      cb[c] = bin;  // beta_in of segment 0
+      __syncthreads();
    }
+   if (NP == 1) __syncthreads();  // every read of the line is complete before it is rewritten
+   cb[me] = sb;
    __syncthreads();
-   const P bin = top ? zero_of<P>() : cb[p * TW + c];
+   const P bin = (p + 1 < NP) ? cb[me + TW] : zero_of<P>();
 
    // ---- forward local recurrence: bt[q] becomes psi'~[lo + q + 1]
-   {
-      P v = zero_of<P>();
+   P v = zero_of<P>();
 #pragma unroll
-      for (int q = 0; q < MSEG; q++) {
-         if (q < K) {
-            const int i = lo + q;
-            const P beta = Op::fma_(Op::ld(tb.M, i), bin, bt[q]);
-            v = Op::fma_(Op::ld(tb.al, i), v, beta);
-            bt[q] = v;
-         }
+   for (int q = 0; q < MSEG; q++) {
+      if (q < K) {
+         const int i = lo + q;
+         const P beta = Op::fma_(Op::ld(t_M, i), bin, bt[q]);
+         v = Op::fma_(Op::ld(t_al, i), v, beta);
+         bt[q] = v;
       }
-      cf[p * TW + c] = v;  // psi'~[hf + 1]
    }
-   __syncthreads();
-   if (p == 0) {
-      P fin = zero_of<P>();  // psi'[0] = 0
-      for (int pp = 1; pp < NP; pp++) {
-         const int lop = pp * m;
-         const P nf = Op::fma_(Op::ld(tb.N, lop), fin, cf[(pp - 1) * TW + c]);
-         cf[(pp - 1) * TW + c] = fin;
-         fin = nf;
+   // ---- prefix scan of the forward maps
+   sa = Op::ld(t_N, hf + 1);
+   sb = v;
+   __syncthreads();  // cb reads above are complete
+   for (int dd = 1; dd < NP; dd <<= 1) {
+      ca[me] = sa;
+      cb[me] = sb;
+      __syncthreads();
+      if (p - dd >= 0) {
+         const P a2 = ca[me - dd * TW], b2 = cb[me - dd * TW];
+         sb = Op::fma_(sa, b2, sb);
+         sa = Op::mul(sa, a2);
       }
-      cf[(NP - 1) * TW + c] = fin;
+      __syncthreads();
    }
+   cb[me] = sb;
    __syncthreads();
-   const P fin = cf[p * TW + c];
+   const P fin = (p >= 1) ? cb[me - TW] : zero_of<P>();  // psi'[lo]
    double acc = 0.;
 #pragma unroll
    for (int q = 0; q < MSEG; q++) {
       if (q < K) {
          const int k = lo + q + 1;
-         const P v = Op::fma_(Op::ld(tb.N, k), fin, bt[q]);
-         line[k * es] = v;
-         if (simp_w) acc += simp_w[k] * (double) dens2(v);
+         const P val = Op::fma_(Op::ld(t_N, k), fin, bt[q]);
+         line[k * es] = val;
+         if (simp_w) acc += simp_w[k] * (double) dens2(val);
       }
    }
    if (p == 0) line[0] = zero_of<P>();
    if (top) line[(n - 1) * es] = zero_of<P>();
    if (simp) *simp = acc;
+}
+
+// Bytes of the four axis tables staged in shared memory.
+template <bool CPLX> __host__ __device__ __forceinline__ int seg_table_bytes(int n) { return 4 * n * (CPLX ? 16 : 8); }
+
+// Issues the bulk copies of the axis tables (alpha, gamma, M, N; n entries
+// each) into shared memory on bar.  Returns the byte count.
+template <bool CPLX> __device__ __forceinline__ uint32_t load_tables(unsigned char *dst, const SegTab &tb, uint64_t *bar) {
+   const uint32_t b = (uint32_t) (tb.n * (CPLX ? 16 : 8));
+   bulk_load(dst, tb.al, b, bar);
+   bulk_load(dst + b, tb.ga, b, bar);
+   bulk_load(dst + 2 * b, tb.M, b, bar);
+   bulk_load(dst + 3 * b, tb.N, b, bar);
+   return 4 * b;
 }
 
 // ---------------------------------------------------------------------------
@@ -168,18 +198,21 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
 // first applies the pending 1/norm and calcnu to the tile (needs phi).
 template <class R, bool CPLX, int AXIS, bool NU, int MSEG>
 __global__ void __launch_bounds__(256, 2) k_sweep_xy(const __grid_constant__ CUtensorMap tm_psi,
-                                                  const __grid_constant__ CUtensorMap tm_phi, Dims d, SegTab tb,
-                                                  Trap trap, double g, double gd, double dt,
-                                                  const State *__restrict__ st, int TW, int boxn, int nbox,
-                                                  uint32_t *err) {
+                                                     const __grid_constant__ CUtensorMap tm_phi, Dims d, SegTab tb,
+                                                     Trap trap, double g, double gd, double dt,
+                                                     const State *__restrict__ st, int TW, int boxn, int nbox,
+                                                     uint32_t *err) {
    using P = typename Tr<R, CPLX>::P;
    extern __shared__ __align__(16) unsigned char smem_raw[];
    __shared__ __align__(8) uint64_t bar;
    const int n = tb.n;
    const int rows = boxn * nbox;  // rows staged (>= n)
-   P *tile = (P *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);  // TMA destinations: 128-byte aligned
+   // layout: tile | phi tile | tables | carry a | carry b  (TMA targets 128-byte aligned)
+   P *tile = (P *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
    R *ptile = (R *) (tile + rows * TW);
-   P *carry = (P *) (((uintptr_t) (ptile + (NU ? rows * TW : 0)) + 15) & ~(uintptr_t) 15);
+   unsigned char *tabs = (unsigned char *) (ptile + (NU ? rows * TW : 0));
+   P *ca = (P *) (tabs + seg_table_bytes<CPLX>(n));
+   P *cb = ca + tb.P * TW;
    const int nzb = (d.nz + TW - 1) / TW;
    const int other = blockIdx.x / nzb;  // y for the x sweep, x for the y sweep
    const int z0 = (blockIdx.x - other * nzb) * TW;
@@ -192,7 +225,8 @@ __global__ void __launch_bounds__(256, 2) k_sweep_xy(const __grid_constant__ CUt
    }
    __syncthreads();
    if (threadIdx.x == 0) {
-      mbar_arrive_expect_tx(&bar, psi_bytes + phi_bytes);
+      mbar_arrive_expect_tx(&bar, psi_bytes + phi_bytes + (uint32_t) seg_table_bytes<CPLX>(n));
+      load_tables<CPLX>(tabs, tb, &bar);
       for (int b = 0; b < nbox; b++) {
          const int a0 = b * boxn;
          if (AXIS == 0) tma_load_3d(tile + a0 * TW, &tm_psi, E * z0, other, a0, &bar);
@@ -219,7 +253,7 @@ __global__ void __launch_bounds__(256, 2) k_sweep_xy(const __grid_constant__ CUt
       __syncthreads();
    }
    const int c = threadIdx.x % TW, p = threadIdx.x / TW;
-   seg_sweep<R, CPLX, MSEG>(tile, TW, 1, c, p, TW, tb, carry, nullptr, nullptr);
+   seg_sweep<R, CPLX, MSEG>(tile, TW, 1, c, p, TW, tb, tabs, ca, cb, nullptr, nullptr);
    fence_proxy_async();
    __syncthreads();
    if (threadIdx.x == 0) {
@@ -240,14 +274,17 @@ __global__ void __launch_bounds__(256, 2) k_sweep_xy(const __grid_constant__ CUt
 // norm of the step.
 template <class R, bool CPLX, bool SIMP, int MSEG>
 __global__ void __launch_bounds__(256, 2) k_sweep_z(typename Tr<R, CPLX>::P *__restrict__ psi, Dims d, SegTab tb,
-                                                 int TR, int LS, const double *__restrict__ wz, double hz3,
-                                                 double *__restrict__ rowsum, uint32_t *err) {
+                                                    int TR, int LS, const double *__restrict__ wz, double hz3,
+                                                    double *__restrict__ rowsum, uint32_t *err) {
    using P = typename Tr<R, CPLX>::P;
    extern __shared__ __align__(16) unsigned char smem_raw[];
    __shared__ __align__(8) uint64_t bar;
+   // layout: rows (stride LS) | tables | carry a | carry b | Simpson partials
    P *tile = (P *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
-   P *carry = tile + TR * LS;
-   double *part = (double *) (carry + 2 * tb.P * TR);
+   unsigned char *tabs = (unsigned char *) (tile + TR * LS);
+   P *ca = (P *) (tabs + seg_table_bytes<CPLX>(tb.n));
+   P *cb = ca + tb.P * TR;
+   double *part = (double *) (cb + tb.P * TR);
    const int nz = d.nz;
    const long long r0 = (long long) blockIdx.x * TR;
    const int nr = (int) ((d.nxy - r0) < TR ? (d.nxy - r0) : TR);
@@ -258,7 +295,8 @@ __global__ void __launch_bounds__(256, 2) k_sweep_z(typename Tr<R, CPLX>::P *__r
    }
    __syncthreads();
    if (threadIdx.x == 0) {
-      mbar_arrive_expect_tx(&bar, row_bytes * nr);
+      mbar_arrive_expect_tx(&bar, row_bytes * nr + (uint32_t) seg_table_bytes<CPLX>(tb.n));
+      load_tables<CPLX>(tabs, tb, &bar);
       for (int r = 0; r < nr; r++) bulk_load(tile + r * LS, psi + (r0 + r) * nz, row_bytes, &bar);
    }
    // rows beyond the grid (last tile) are zero so their sweep stays finite
@@ -266,7 +304,7 @@ __global__ void __launch_bounds__(256, 2) k_sweep_z(typename Tr<R, CPLX>::P *__r
    if (__syncthreads_or(!mbar_wait(&bar, 0, err))) return;
    const int c = threadIdx.x % TR, p = threadIdx.x / TR;
    double my = 0.;
-   seg_sweep<R, CPLX, MSEG>(tile, 1, LS, c, p, TR, tb, carry, SIMP ? wz : nullptr, SIMP ? &my : nullptr);
+   seg_sweep<R, CPLX, MSEG>(tile, 1, LS, c, p, TR, tb, tabs, ca, cb, SIMP ? wz : nullptr, SIMP ? &my : nullptr);
    if (SIMP) part[p * TR + c] = my;
    fence_proxy_async();
    __syncthreads();
