@@ -38,6 +38,24 @@ __host__ __device__ __forceinline__ float csub_any(float a, float b) { return a 
 __host__ __device__ __forceinline__ double2 csub_any(double2 a, double2 b) { return csub(a, b); }
 __host__ __device__ __forceinline__ float2 csub_any(float2 a, float2 b) { return csub(a, b); }
 
+// warp shuffles of real or complex elements
+__device__ __forceinline__ double shfl_down_any(unsigned m, double v, int d) { return __shfl_down_sync(m, v, d); }
+__device__ __forceinline__ float shfl_down_any(unsigned m, float v, int d) { return __shfl_down_sync(m, v, d); }
+__device__ __forceinline__ double2 shfl_down_any(unsigned m, double2 v, int d) {
+   return make_double2(__shfl_down_sync(m, v.x, d), __shfl_down_sync(m, v.y, d));
+}
+__device__ __forceinline__ float2 shfl_down_any(unsigned m, float2 v, int d) {
+   return make_float2(__shfl_down_sync(m, v.x, d), __shfl_down_sync(m, v.y, d));
+}
+__device__ __forceinline__ double shfl_up_any(unsigned m, double v, int d) { return __shfl_up_sync(m, v, d); }
+__device__ __forceinline__ float shfl_up_any(unsigned m, float v, int d) { return __shfl_up_sync(m, v, d); }
+__device__ __forceinline__ double2 shfl_up_any(unsigned m, double2 v, int d) {
+   return make_double2(__shfl_up_sync(m, v.x, d), __shfl_up_sync(m, v.y, d));
+}
+__device__ __forceinline__ float2 shfl_up_any(unsigned m, float2 v, int d) {
+   return make_float2(__shfl_up_sync(m, v.x, d), __shfl_up_sync(m, v.y, d));
+}
+
 // psi element: real R in imaginary time, complex in real time
 template <class R, bool CPLX> struct psi_elem { using type = R; };
 template <class R> struct psi_elem<R, true> { using type = cpx<R>; };

@@ -88,6 +88,7 @@ struct gpe_solver {
       void *M = nullptr, *N = nullptr;
    } sw[3];
    double *wz = nullptr;      // Simpson weights along z (norm partials)
+   int nsm = 148;             // streaming multiprocessors of the device
    uint32_t *err = nullptr;   // device status word (bounded waits)
    // per-kernel profiling: when prof_ev is set, mark() records an event
    // after every kernel of a step
@@ -115,12 +116,6 @@ static bool make_plan(int n, FftPlan &pl) {
       ns *= pl.rad[st];
    }
    return m == 1;
-}
-
-static int floor_pow2(long long v) {
-   int r = 1;
-   while ((long long) r * 2 <= v) r *= 2;
-   return r;
 }
 
 static gpe_status validate(const gpe_params *p) {
@@ -320,15 +315,18 @@ static gpe_status make_tmap(CUtensorMap *m, void *base, size_t esz, long w_nz, l
 }
 
 // Lines per CTA and segment length for a sweep over lines of length n with
-// `tw_base` lines filling a 128-byte row: at most 256 threads per CTA.
-static void pick_sweep(int n, int tw_base, int &TW, int &MSEG, int &P) {
+// `tw_base` lines filling a 128-byte row: at most 256 threads per CTA.  Lines
+// of 16-byte elements keep 8-point segments (16 would spill registers at
+// three CTAs per SM) and narrow the tile instead.
+static void pick_sweep(int n, int tw_base, bool wide, int &TW, int &MSEG, int &P) {
    const int ms[2] = {8, 16};
+   const int nms = wide ? 1 : 2;
    for (int tw = tw_base; tw >= 2; tw /= 2)
-      for (int mi = 0; mi < 2; mi++) {
+      for (int mi = 0; mi < nms; mi++) {
          const int p = (n - 2 + ms[mi] - 1) / ms[mi];
          if (tw * p <= 256) { TW = tw; MSEG = ms[mi]; P = p; return; }
       }
-   TW = 2; MSEG = 16; P = (n - 2 + 15) / 16;
+   TW = 2; MSEG = wide ? 8 : 16; P = (n - 2 + MSEG - 1) / MSEG;
 }
 
 static gpe_status setup_sweeps(gpe_solver *s) {
@@ -341,10 +339,10 @@ static gpe_status setup_sweeps(gpe_solver *s) {
    for (int ax = 0; ax < 3; ax++) {
       auto &w = s->sw[ax];
       int P = 1;
-      pick_sweep((int) nn[ax], tw_base, w.TW, w.MSEG, P);
+      pick_sweep((int) nn[ax], tw_base, esz == 16, w.TW, w.MSEG, P);
       CKS(make_segtab(s, ax, nn[ax], h2[ax], w.MSEG, P));
-      const size_t carry = 2 * (size_t) P * w.TW * esz;
-      const size_t tabs = (size_t) 4 * nn[ax] * (s->cplx ? 16 : 8);
+      const int spw = 32 / w.TW;
+      const size_t blk = 2 * (size_t) ((P + spw - 1) / spw + 1) * w.TW * esz;
       if (ax < 2) {
          w.boxn = (int) std::min<long>(nn[ax], 256);
          w.nbox = (int) ((nn[ax] + w.boxn - 1) / w.boxn);
@@ -352,11 +350,12 @@ static gpe_status setup_sweeps(gpe_solver *s) {
          const int by = ax == 1 ? w.boxn : 1, bx = ax == 0 ? w.boxn : 1;
          CKS(make_tmap(&w.tm_psi, s->psi, s->fp32 ? 4 : 8, E * d.nz, d.ny, d.nx, E * w.TW, by, bx));
          CKS(make_tmap(&w.tm_phi, s->phi, rsz, d.nz, d.ny, d.nx, w.TW, by, bx));
-         w.smem = 128 + rows * w.TW * esz + (ax == 0 ? rows * w.TW * rsz : 0) + tabs + carry;
+         w.smem = 128 + rows * w.TW * esz + (ax == 0 ? rows * w.TW * rsz : 0) + 16 + blk;
       } else {
          w.LS = (int) (d.nz + 16 / esz);
-         w.smem = 128 + (size_t) w.TW * w.LS * esz + tabs + carry + (size_t) P * w.TW * sizeof(double);
+         w.smem = 128 + (size_t) w.TW * w.LS * esz + blk + (size_t) P * w.TW * sizeof(double);
       }
+      if (w.smem > 227 * 1024) return fail(GPE_ERR_PARAM, "grid too large for the sweep tiles (shared memory)");
    }
    // spectrum tiles: spec[x][y][kz] viewed as [nx][ny][2 nzh] scalars
    {
@@ -433,6 +432,7 @@ static gpe_status create_impl(const gpe_params *p, void *stream, gpe_solver *s) 
    s->par = (p->opt == 2) ? 2. : 1.;
    if (p->device >= 0) CK(cudaSetDevice(p->device));
    CK(cudaGetDevice(&s->dev));
+   CK(cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, s->dev));
    if (stream) {
       s->st = (cudaStream_t) stream;
    } else {
@@ -595,7 +595,7 @@ template <class R, bool CPLX> struct Impl {
       CKS(smem_attr(f, w.smem));
       const int nzb = (d.nz + w.TW - 1) / w.TW;
       const unsigned grid = (unsigned) ((AXIS == 0 ? d.ny : d.nx) * nzb);
-      k_sweep_xy<R, CPLX, AXIS, NU, MSEG><<<grid, w.TW * w.tab.P, w.smem, s->st>>>(
+      k_sweep_xy<R, CPLX, AXIS, NU, MSEG><<<grid, ((w.TW * w.tab.P + 31) & ~31), w.smem, s->st>>>(
           w.tm_psi, w.tm_phi, d, w.tab, trap_of(s), g, gd, s->p.dt, s->state, w.TW, w.boxn, w.nbox, s->err);
       CKL();
       mark(s);
@@ -620,7 +620,7 @@ template <class R, bool CPLX> struct Impl {
       const Dims &d = s->d;
       const void *f = (const void *) k_sweep_z<R, CPLX, SIMP, MSEG>;
       CKS(smem_attr(f, w.smem));
-      k_sweep_z<R, CPLX, SIMP, MSEG><<<blocks_for(d.nxy, w.TW), w.TW * w.tab.P, w.smem, s->st>>>(
+      k_sweep_z<R, CPLX, SIMP, MSEG><<<blocks_for(d.nxy, w.TW), ((w.TW * w.tab.P + 31) & ~31), w.smem, s->st>>>(
           (P *) s->psi, d, w.tab, w.TW, w.LS, s->wz, s->p.dz / 3., s->rowA, s->err);
       CKL();
       mark(s);

@@ -5,7 +5,8 @@
 // A CTA owns TW lines.  The lines are brought in by one TMA tensor load (x
 // and y sweeps: box of TW z-columns by the whole line) or by one bulk copy
 // per row (z sweep), so every HBM access is a full 128-byte row segment and
-// no transpose is needed.  Each line is split into P segments of m points,
+// no transpose is needed.  The per-axis coefficient tables are read through
+// the L1 cache, which the CTAs of an SM share.  Each line is split into P segments of m points,
 // one thread per (line, segment); the two first-order recurrences of the
 // Thomas algorithm
 //    beta[i-1] = gamma[i] (A beta[i] - c_i),      i = n-2 .. 1
@@ -34,10 +35,10 @@ template <class R, bool CPLX> struct SegOps {
    using P = typename Tr<R, CPLX>::P;
    __device__ static P ld(const void *t, int i) {
       if constexpr (CPLX) {
-         const double2 v = ((const double2 *) t)[i];
+         const double2 v = __ldg((const double2 *) t + i);
          return mk<R>((R) v.x, (R) v.y);
       } else {
-         return (R) ((const double *) t)[i];
+         return (R) __ldg((const double *) t + i);
       }
    }
    __device__ static P cv(double2 v) {
@@ -64,28 +65,29 @@ template <class R, bool CPLX> struct SegOps {
 
 // Segmented Thomas sweep of line c held in shared memory at
 // s[i * es + c * cs], i in [0, n).  Called by all threads of the CTA; thread
-// (c, p) owns recurrence indices [p m, hf].  tabs points to the axis tables
-// staged in shared memory: alpha, gamma, M, N, n entries each.  ca and cb are
-// shared scratch of P * TW elements each.  Writes the swept line back in
-// place.  When simp_w is non-null, *simp receives this thread's share of
-// sum_i simp_w[i] |psi'_i|^2.
+// t = p * TW + c owns recurrence indices [p m, hf] of line c.  A warp holds
+// SPW = 32 / TW consecutive segments of each of its TW lines.  blk is a
+// shared scratch of 2 * (NW + 1) * TW elements (NW warps hold segments).
+// Writes the swept line back in place.  When simp_w is non-null, *simp
+// receives this thread's share of sum_i simp_w[i] |psi'_i|^2.
 //
 // Carries: segment p maps the value entering at its top (index hf+1) to the
 // value at its bottom (index lo) by the affine map x -> b + a x with
 // a = M[lo], b = beta~[lo]; the value entering segment p is the composition
-// of the maps of all segments above it (a suffix scan, Kogge-Stone in log2 P
-// rounds).  The forward recurrence composes x -> psi'~[hf+1] + N[hf+1] x from
-// the bottom (a prefix scan).
+// of the maps of all segments above it: a suffix scan, done with shuffles
+// inside a warp and a short chain over the warps above.  The forward
+// recurrence composes x -> psi'~[hf+1] + N[hf+1] x from the bottom (prefix).
 template <class R, bool CPLX, int MSEG>
 __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, int cs, int c, int p, int TW,
-                                          const SegTab &tb, const unsigned char *tabs,
-                                          typename Tr<R, CPLX>::P *ca, typename Tr<R, CPLX>::P *cb,
-                                          const double *simp_w, double *simp) {
+                                          const SegTab &tb, typename Tr<R, CPLX>::P *blk, const double *simp_w,
+                                          double *simp) {
    using Op = SegOps<R, CPLX>;
    using P = typename Tr<R, CPLX>::P;
-   constexpr int TE = CPLX ? 16 : 8;  // bytes of one table entry (double or double2)
    const int n = tb.n, m = tb.m, NP = tb.P;
-   const void *t_al = tabs, *t_ga = tabs + n * TE, *t_M = tabs + 2 * n * TE, *t_N = tabs + 3 * n * TE;
+   const int SPW = 32 / TW;              // segments of one line inside a warp
+   const int NW = (NP + SPW - 1) / SPW;  // warps that hold segments
+   const int lane = threadIdx.x & 31, j = lane / TW, w = threadIdx.x >> 5;
+   const bool act = p < NP;
    const int lo = p * m;
    const bool top = (p == NP - 1);
    const int hf = top ? n - 3 : lo + m - 1;  // last owned recurrence index
@@ -93,11 +95,12 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
    const P A = Op::cv(tb.A), A0r = Op::cv(tb.A0r), mA = Op::cv(tb.mA);
    P *line = s + c * cs;
    auto L = [&](int i) -> P { return line[i * es]; };
-   const int me = p * TW + c;
+   P *ba = blk, *bb = blk + (NW + 1) * TW;  // per-warp block maps [NW][TW]
+   const unsigned fullmask = 0xffffffffu;
 
    // ---- backward local recurrence: bt[q] = beta~[lo + q]
    P bt[MSEG];
-   {
+   if (act) {
       P b = top ? L(n - 1) : zero_of<P>();  // beta[n-2] = psi[n-1] is exact
       // the step producing beta[lo+q] uses i = lo+q+1: psi[i+1], psi[i], psi[i-1]
       P w2 = L(lo + K + 1);
@@ -109,95 +112,103 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
             P cc = Op::mul(mA, w2);
             cc = cadd_any(cc, Op::mul(A0r, w1));
             cc = csub_any(cc, Op::mul(A, w0));
-            b = Op::mul(Op::ld(t_ga, lo + q + 1), csub_any(Op::mul(A, b), cc));
+            b = Op::mul(Op::ld(tb.ga, lo + q + 1), csub_any(Op::mul(A, b), cc));
             bt[q] = b;
             w2 = w1;
             w1 = w0;
          }
       }
    }
-   // ---- suffix scan of the backward maps
-   P sa = top ? zero_of<P>() : Op::ld(t_M, lo), sb = bt[0];
-   for (int dd = 1; dd < NP; dd <<= 1) {
-      ca[me] = sa;
-      cb[me] = sb;
-      __syncthreads();
-      if (p + dd < NP) {
-         const P a2 = ca[me + dd * TW], b2 = cb[me + dd * TW];
+   // ---- suffix scan of the backward maps: in-warp, then over the warps above
+   P sa = zero_of<P>(), sb = zero_of<P>();
+   if (act) {
+      sa = top ? zero_of<P>() : Op::ld(tb.M, lo);
+      sb = bt[0];
+   }
+   for (int dd = 1; dd < SPW; dd <<= 1) {
+      const P a2 = shfl_down_any(fullmask, sa, dd * TW), b2 = shfl_down_any(fullmask, sb, dd * TW);
+      if (j + dd < SPW && p + dd < NP) {
          sb = Op::fma_(sa, b2, sb);
          sa = Op::mul(sa, a2);
       }
-      __syncthreads();
    }
-   if (NP == 1) __syncthreads();  // every read of the line is complete before it is rewritten
-   cb[me] = sb;
-   __syncthreads();
-   const P bin = (p + 1 < NP) ? cb[me + TW] : zero_of<P>();
+   if (j == 0 && w < NW) {
+      ba[w * TW + c] = sa;
+      bb[w * TW + c] = sb;
+   }
+   __syncthreads();  // also: every read of the line is complete before it is rewritten
+   P bin = zero_of<P>();
+   {
+      // value entering the top segment of this warp from the warps above
+      P x = zero_of<P>();
+      for (int ww = NW - 1; ww > w; ww--) x = Op::fma_(ba[ww * TW + c], x, bb[ww * TW + c]);
+      const P here = Op::fma_(sa, x, sb);  // beta at the bottom of this segment
+      const P nxt = shfl_down_any(fullmask, here, TW);
+      bin = (j + 1 < SPW) ? nxt : x;
+      if (!act || top) bin = zero_of<P>();
+   }
+   __syncthreads();  // the block maps are reused below
 
    // ---- forward local recurrence: bt[q] becomes psi'~[lo + q + 1]
    P v = zero_of<P>();
+   sa = zero_of<P>();
+   if (act) {
 #pragma unroll
-   for (int q = 0; q < MSEG; q++) {
-      if (q < K) {
-         const int i = lo + q;
-         const P beta = Op::fma_(Op::ld(t_M, i), bin, bt[q]);
-         v = Op::fma_(Op::ld(t_al, i), v, beta);
-         bt[q] = v;
+      for (int q = 0; q < MSEG; q++) {
+         if (q < K) {
+            const int i = lo + q;
+            const P beta = Op::fma_(Op::ld(tb.M, i), bin, bt[q]);
+            v = Op::fma_(Op::ld(tb.al, i), v, beta);
+            bt[q] = v;
+         }
       }
+      sa = Op::ld(tb.N, hf + 1);
    }
    // ---- prefix scan of the forward maps
-   sa = Op::ld(t_N, hf + 1);
    sb = v;
-   __syncthreads();  // cb reads above are complete
-   for (int dd = 1; dd < NP; dd <<= 1) {
-      ca[me] = sa;
-      cb[me] = sb;
-      __syncthreads();
-      if (p - dd >= 0) {
-         const P a2 = ca[me - dd * TW], b2 = cb[me - dd * TW];
+   for (int dd = 1; dd < SPW; dd <<= 1) {
+      const P a2 = shfl_up_any(fullmask, sa, dd * TW), b2 = shfl_up_any(fullmask, sb, dd * TW);
+      if (j >= dd) {
          sb = Op::fma_(sa, b2, sb);
          sa = Op::mul(sa, a2);
       }
-      __syncthreads();
    }
-   cb[me] = sb;
+   if (j == SPW - 1 && w < NW) {
+      ba[w * TW + c] = sa;
+      bb[w * TW + c] = sb;
+   }
    __syncthreads();
-   const P fin = (p >= 1) ? cb[me - TW] : zero_of<P>();  // psi'[lo]
    double acc = 0.;
+   {
+      P x = zero_of<P>();  // psi' entering the first segment of this warp
+      for (int ww = 0; ww < w; ww++) x = Op::fma_(ba[ww * TW + c], x, bb[ww * TW + c]);
+      const P upto = Op::fma_(sa, x, sb);  // psi'[hf + 1] of this segment
+      const P prv = shfl_up_any(fullmask, upto, TW);
+      const P fin = (j >= 1) ? prv : x;  // psi'[lo]
+      if (act) {
 #pragma unroll
-   for (int q = 0; q < MSEG; q++) {
-      if (q < K) {
-         const int k = lo + q + 1;
-         const P val = Op::fma_(Op::ld(t_N, k), fin, bt[q]);
-         line[k * es] = val;
-         if (simp_w) acc += simp_w[k] * (double) dens2(val);
+         for (int q = 0; q < MSEG; q++) {
+            if (q < K) {
+               const int k = lo + q + 1;
+               const P val = Op::fma_(Op::ld(tb.N, k), fin, bt[q]);
+               line[k * es] = val;
+               if (simp_w) acc += simp_w[k] * (double) dens2(val);
+            }
+         }
+         if (p == 0) line[0] = zero_of<P>();
+         if (top) line[(n - 1) * es] = zero_of<P>();
       }
    }
-   if (p == 0) line[0] = zero_of<P>();
-   if (top) line[(n - 1) * es] = zero_of<P>();
    if (simp) *simp = acc;
-}
-
-// Bytes of the four axis tables staged in shared memory.
-template <bool CPLX> __host__ __device__ __forceinline__ int seg_table_bytes(int n) { return 4 * n * (CPLX ? 16 : 8); }
-
-// Issues the bulk copies of the axis tables (alpha, gamma, M, N; n entries
-// each) into shared memory on bar.  Returns the byte count.
-template <bool CPLX> __device__ __forceinline__ uint32_t load_tables(unsigned char *dst, const SegTab &tb, uint64_t *bar) {
-   const uint32_t b = (uint32_t) (tb.n * (CPLX ? 16 : 8));
-   bulk_load(dst, tb.al, b, bar);
-   bulk_load(dst + b, tb.ga, b, bar);
-   bulk_load(dst + 2 * b, tb.M, b, bar);
-   bulk_load(dst + 3 * b, tb.N, b, bar);
-   return 4 * b;
 }
 
 // ---------------------------------------------------------------------------
 // x or y sweep.  Tile: TW consecutive z columns of one y (x sweep) or one x
-// (y sweep) plane, the whole line along the swept axis.  With NU the x sweep
-// first applies the pending 1/norm and calcnu to the tile (needs phi).
+// (y sweep) plane, the whole line along the swept axis, brought in by TMA.
+// With NU the x sweep first applies the pending 1/norm and calcnu to the tile
+// (needs phi).
 template <class R, bool CPLX, int AXIS, bool NU, int MSEG>
-__global__ void __launch_bounds__(256, 2) k_sweep_xy(const __grid_constant__ CUtensorMap tm_psi,
+__global__ void __launch_bounds__(256, 3) k_sweep_xy(const __grid_constant__ CUtensorMap tm_psi,
                                                      const __grid_constant__ CUtensorMap tm_phi, Dims d, SegTab tb,
                                                      Trap trap, double g, double gd, double dt,
                                                      const State *__restrict__ st, int TW, int boxn, int nbox,
@@ -207,12 +218,10 @@ __global__ void __launch_bounds__(256, 2) k_sweep_xy(const __grid_constant__ CUt
    __shared__ __align__(8) uint64_t bar;
    const int n = tb.n;
    const int rows = boxn * nbox;  // rows staged (>= n)
-   // layout: tile | phi tile | tables | carry a | carry b  (TMA targets 128-byte aligned)
+   // layout: tile | phi tile | block maps  (TMA targets 128-byte aligned)
    P *tile = (P *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
    R *ptile = (R *) (tile + rows * TW);
-   unsigned char *tabs = (unsigned char *) (ptile + (NU ? rows * TW : 0));
-   P *ca = (P *) (tabs + seg_table_bytes<CPLX>(n));
-   P *cb = ca + tb.P * TW;
+   P *blk = (P *) (((uintptr_t) (ptile + (NU ? rows * TW : 0)) + 15) & ~(uintptr_t) 15);
    const int nzb = (d.nz + TW - 1) / TW;
    const int other = blockIdx.x / nzb;  // y for the x sweep, x for the y sweep
    const int z0 = (blockIdx.x - other * nzb) * TW;
@@ -225,8 +234,7 @@ __global__ void __launch_bounds__(256, 2) k_sweep_xy(const __grid_constant__ CUt
    }
    __syncthreads();
    if (threadIdx.x == 0) {
-      mbar_arrive_expect_tx(&bar, psi_bytes + phi_bytes + (uint32_t) seg_table_bytes<CPLX>(n));
-      load_tables<CPLX>(tabs, tb, &bar);
+      mbar_arrive_expect_tx(&bar, psi_bytes + phi_bytes);
       for (int b = 0; b < nbox; b++) {
          const int a0 = b * boxn;
          if (AXIS == 0) tma_load_3d(tile + a0 * TW, &tm_psi, E * z0, other, a0, &bar);
@@ -253,7 +261,7 @@ __global__ void __launch_bounds__(256, 2) k_sweep_xy(const __grid_constant__ CUt
       __syncthreads();
    }
    const int c = threadIdx.x % TW, p = threadIdx.x / TW;
-   seg_sweep<R, CPLX, MSEG>(tile, TW, 1, c, p, TW, tb, tabs, ca, cb, nullptr, nullptr);
+   seg_sweep<R, CPLX, MSEG>(tile, TW, 1, c, p, TW, tb, blk, nullptr, nullptr);
    fence_proxy_async();
    __syncthreads();
    if (threadIdx.x == 0) {
@@ -267,24 +275,22 @@ __global__ void __launch_bounds__(256, 2) k_sweep_xy(const __grid_constant__ CUt
    }
 }
 
-// ---------------------------------------------------------------------------
 // z sweep.  Tile: TR consecutive (x, y) rows, each copied by one bulk copy to
 // a padded shared row (stride LS elements).  With SIMP every row also yields
 // its Simpson integral of |psi'|^2 (simpint over z, diffint.cu:106) for the
 // norm of the step.
 template <class R, bool CPLX, bool SIMP, int MSEG>
-__global__ void __launch_bounds__(256, 2) k_sweep_z(typename Tr<R, CPLX>::P *__restrict__ psi, Dims d, SegTab tb,
+__global__ void __launch_bounds__(256, 3) k_sweep_z(typename Tr<R, CPLX>::P *__restrict__ psi, Dims d, SegTab tb,
                                                     int TR, int LS, const double *__restrict__ wz, double hz3,
                                                     double *__restrict__ rowsum, uint32_t *err) {
    using P = typename Tr<R, CPLX>::P;
    extern __shared__ __align__(16) unsigned char smem_raw[];
    __shared__ __align__(8) uint64_t bar;
-   // layout: rows (stride LS) | tables | carry a | carry b | Simpson partials
+   // layout: rows (stride LS) | block maps | Simpson partials
    P *tile = (P *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
-   unsigned char *tabs = (unsigned char *) (tile + TR * LS);
-   P *ca = (P *) (tabs + seg_table_bytes<CPLX>(tb.n));
-   P *cb = ca + tb.P * TR;
-   double *part = (double *) (cb + tb.P * TR);
+   const int NW = (tb.P + 32 / TR - 1) / (32 / TR);
+   P *blk = tile + TR * LS;
+   double *part = (double *) (blk + 2 * (NW + 1) * TR);
    const int nz = d.nz;
    const long long r0 = (long long) blockIdx.x * TR;
    const int nr = (int) ((d.nxy - r0) < TR ? (d.nxy - r0) : TR);
@@ -295,8 +301,7 @@ __global__ void __launch_bounds__(256, 2) k_sweep_z(typename Tr<R, CPLX>::P *__r
    }
    __syncthreads();
    if (threadIdx.x == 0) {
-      mbar_arrive_expect_tx(&bar, row_bytes * nr + (uint32_t) seg_table_bytes<CPLX>(tb.n));
-      load_tables<CPLX>(tabs, tb, &bar);
+      mbar_arrive_expect_tx(&bar, row_bytes * nr);
       for (int r = 0; r < nr; r++) bulk_load(tile + r * LS, psi + (r0 + r) * nz, row_bytes, &bar);
    }
    // rows beyond the grid (last tile) are zero so their sweep stays finite
@@ -304,8 +309,8 @@ __global__ void __launch_bounds__(256, 2) k_sweep_z(typename Tr<R, CPLX>::P *__r
    if (__syncthreads_or(!mbar_wait(&bar, 0, err))) return;
    const int c = threadIdx.x % TR, p = threadIdx.x / TR;
    double my = 0.;
-   seg_sweep<R, CPLX, MSEG>(tile, 1, LS, c, p, TR, tb, tabs, ca, cb, SIMP ? wz : nullptr, SIMP ? &my : nullptr);
-   if (SIMP) part[p * TR + c] = my;
+   seg_sweep<R, CPLX, MSEG>(tile, 1, LS, c, p, TR, tb, blk, SIMP ? wz : nullptr, SIMP ? &my : nullptr);
+   if (SIMP && p < tb.P) part[p * TR + c] = my;
    fence_proxy_async();
    __syncthreads();
    if (SIMP && p == 0 && c < nr) {

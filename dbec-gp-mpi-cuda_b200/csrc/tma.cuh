@@ -43,6 +43,30 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
    return ok != 0;
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Named barrier 1 over the nthreads consumer threads of a warp-specialised
+// CTA (the producer warp never takes part).
+__device__ __forceinline__ void consumer_sync(int nthreads) {
+   asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
+}
+
+// Consumer barrier that also ORs a flag across the consumer threads.
+__device__ __forceinline__ bool consumer_any(bool flag, int nthreads) {
+   uint32_t r;
+   asm volatile(
+       "{\n\t.reg .pred p, q;\n\t"
+       "setp.ne.u32 p, %1, 0;\n\t"
+       "bar.red.or.pred q, 1, %2, p;\n\t"
+       "selp.u32 %0, 1, 0, q;\n\t}"
+       : "=r"(r)
+       : "r"((uint32_t) flag), "r"(nthreads)
+       : "memory");
+   return r != 0;
+}
+
 // Bounded wait for phase `parity` of `bar`.  Returns false (and sets bit
 // kErrTmaTimeout in *err) when the copy did not complete in time.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t *err) {
