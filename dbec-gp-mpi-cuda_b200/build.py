@@ -27,8 +27,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
                   "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC]
 
-LIB_SOURCES = ["solver.cu"]
-LIB_DEPS = ["solver.cu", "common.cuh", "fft.cuh", "kernels.cuh", "step_kernels.cuh", "sweep_kernels.cuh", "tma.cuh"]
+LIB_SOURCES = ["solver.cu", "noalloc.cu"]
+LIB_DEPS = ["solver.cu", "noalloc.cu", "common.cuh", "fft.cuh", "kernels.cuh", "step_kernels.cuh", "sweep_kernels.cuh", "tma.cuh"]
 HOST_COMMON = ["cfg.cpp", "cli.cpp"]
 PROGRAMS = {"imag3d-mpicuda": "imag3d_main.cpp", "real3d-mpicuda": "real3d_main.cpp"}
 

@@ -25,6 +25,10 @@ static const double kRefPi = 3.14159265358979;
 
 static thread_local std::string g_err;
 
+namespace gpe {
+void set_last_error(const std::string &msg) { g_err = msg; }
+}  // namespace gpe
+
 static gpe_status fail(gpe_status st, const std::string &msg) {
    g_err = msg;
    return st;

@@ -67,6 +67,7 @@ _SIGS = {
     "gpe_profile_step": (C.c_int, [_P, C.c_long, _D, _D, _P, C.c_int, C.POINTER(C.c_int)]),
     "gpe_step_kernel_name": (C.c_char_p, [_P, C.c_int]),
     "gpe_step_kernel_bytes": (C.c_double, [_P, C.c_int]),
+    "gpe_norm_noalloc": (C.c_int, [_P, C.c_int, C.c_long, C.c_long, C.c_long, _D, _D, _D, _P, _P]),
 }
 
 _lib = None
@@ -103,6 +104,14 @@ def _ptr(a):
 def make_params(mode, nx, ny, nz, dx, dy, dz, dt, gamma, nu, lamda, cutoff, opt=1, precision=PREC_FP64, device=-1):
     return Params(int(mode), int(precision), int(opt), int(device), int(nx), int(ny), int(nz), float(dx), float(dy),
                   float(dz), float(dt), float(gamma), float(nu), float(lamda), float(cutoff))
+
+
+def norm_noalloc(psi_dev_ptr, mode, nx, ny, nz, dx, dy, dz, norm_dev_ptr, stream=None):
+    """Queues the allocation-free norm of a device-resident psi (device
+    pointers as integers); the result lands in *norm_dev_ptr."""
+    _check(lib().gpe_norm_noalloc(C.c_void_p(psi_dev_ptr), int(mode), int(nx), int(ny), int(nz), float(dx),
+                                  float(dy), float(dz), C.c_void_p(norm_dev_ptr),
+                                  C.c_void_p(stream) if stream else None))
 
 
 def device_bytes(params: Params) -> int:

@@ -134,6 +134,21 @@ gpe_status gpe_profile_step(gpe_solver *s, long nsteps, double g, double gd, dou
 const char *gpe_step_kernel_name(gpe_solver *s, int i);
 double gpe_step_kernel_bytes(gpe_solver *s, int i);
 
+/* Norm of a device-resident psi with no device allocation.  No counterpart in
+ * the reference: it serves callers that cannot call cudaMalloc where they need
+ * the norm (a latency-critical loop that must not take cudaMalloc/cudaFree's
+ * implicit synchronisation, or a process whose device memory belongs to
+ * another allocator).  psi_dev: nx*ny*nz doubles (mode GPE_MODE_IMAG) or
+ * interleaved complex doubles (GPE_MODE_REAL), x-major; norm_dev: one device
+ * double that receives sqrt(Simpson integral of |psi|^2), as calcnorm.  Work
+ * is queued on stream (NULL = default stream) and nothing is allocated: the
+ * per-row partials live in a 2 MiB file-scope device array, so nx*ny must be
+ * at most 262144 and nx at most 1024 (GPE_ERR_PARAM otherwise).  The first
+ * call on a device looks up that array's address; make it before any stream
+ * capture.  Calls that overlap on the GPU share the array and race. */
+gpe_status gpe_norm_noalloc(const void *psi_dev, int mode, long nx, long ny, long nz, double dx, double dy, double dz,
+                            double *norm_dev, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
