@@ -85,7 +85,7 @@ struct gpe_solver {
    size_t obs_cap = 0;
    // sweep configuration per axis (x, y: TMA tensor tiles; z: bulk rows)
    struct Sweep {
-      int TW = 8, MSEG = 8, boxn = 0, nbox = 1, LS = 0;
+      int TW = 8, MSEG = 8, boxn = 0, nbox = 1, LS = 0, S = 2, ctas = 1;
       size_t smem = 0;
       CUtensorMap tm_psi{}, tm_phi{};
       SegTab tab{};
@@ -347,6 +347,7 @@ static gpe_status setup_sweeps(gpe_solver *s) {
       CKS(make_segtab(s, ax, nn[ax], h2[ax], w.MSEG, P));
       const int spw = 32 / w.TW;
       const size_t blk = 2 * (size_t) ((P + spw - 1) / spw + 1) * w.TW * esz;
+      size_t stage = 0, fixed = 0;
       if (ax < 2) {
          w.boxn = (int) std::min<long>(nn[ax], 256);
          w.nbox = (int) ((nn[ax] + w.boxn - 1) / w.boxn);
@@ -354,12 +355,19 @@ static gpe_status setup_sweeps(gpe_solver *s) {
          const int by = ax == 1 ? w.boxn : 1, bx = ax == 0 ? w.boxn : 1;
          CKS(make_tmap(&w.tm_psi, s->psi, s->fp32 ? 4 : 8, E * d.nz, d.ny, d.nx, E * w.TW, by, bx));
          CKS(make_tmap(&w.tm_phi, s->phi, rsz, d.nz, d.ny, d.nx, w.TW, by, bx));
-         w.smem = 128 + rows * w.TW * esz + (ax == 0 ? rows * w.TW * rsz : 0) + 16 + blk;
+         stage = (rows * w.TW * esz + (ax == 0 ? rows * w.TW * rsz : 0) + 127) & ~(size_t) 127;
+         fixed = 128 + blk;
       } else {
          w.LS = (int) (d.nz + 16 / esz);
-         w.smem = 128 + (size_t) w.TW * w.LS * esz + blk + (size_t) P * w.TW * sizeof(double);
+         stage = ((size_t) w.TW * w.LS * esz + 127) & ~(size_t) 127;
+         fixed = 128 + blk + (size_t) P * w.TW * sizeof(double);
       }
-      if (w.smem > 227 * 1024) return fail(GPE_ERR_PARAM, "grid too large for the sweep tiles (shared memory)");
+      // pipeline depth: 3 stages when two CTAs still fit on an SM, else 2
+      const size_t sm_cap = 227 * 1024;
+      w.S = (fixed + 3 * stage) * 2 <= sm_cap ? 3 : 2;
+      w.smem = fixed + w.S * stage;
+      if (w.smem > sm_cap) return fail(GPE_ERR_PARAM, "grid too large for the sweep tiles (shared memory)");
+      w.ctas = std::max<int>(1, std::min<int>(2, (int) (sm_cap / w.smem)));
    }
    // spectrum tiles: spec[x][y][kz] viewed as [nx][ny][2 nzh] scalars
    {
@@ -592,14 +600,15 @@ template <class R, bool CPLX> struct Impl {
       return GPE_OK;
    }
 
-   template <int AXIS, bool NU, int MSEG> static gpe_status sweep_xy_launch(gpe_solver *s, double g, double gd) {
+   template <int AXIS, bool NU, int MSEG, int S> static gpe_status sweep_xy_launch(gpe_solver *s, double g, double gd) {
       auto &w = s->sw[AXIS];
       const Dims &d = s->d;
-      const void *f = (const void *) k_sweep_xy<R, CPLX, AXIS, NU, MSEG>;
+      const void *f = (const void *) k_sweep_xy<R, CPLX, AXIS, NU, MSEG, S>;
       CKS(smem_attr(f, w.smem));
       const int nzb = (d.nz + w.TW - 1) / w.TW;
-      const unsigned grid = (unsigned) ((AXIS == 0 ? d.ny : d.nx) * nzb);
-      k_sweep_xy<R, CPLX, AXIS, NU, MSEG><<<grid, ((w.TW * w.tab.P + 31) & ~31), w.smem, s->st>>>(
+      const int ntiles = (AXIS == 0 ? d.ny : d.nx) * nzb;
+      const unsigned grid = (unsigned) std::min(ntiles, w.ctas * s->nsm);
+      k_sweep_xy<R, CPLX, AXIS, NU, MSEG, S><<<grid, ((w.TW * w.tab.P + 31) & ~31), w.smem, s->st>>>(
           w.tm_psi, w.tm_phi, d, w.tab, trap_of(s), g, gd, s->p.dt, s->state, w.TW, w.boxn, w.nbox, s->err);
       CKL();
       mark(s);
@@ -607,24 +616,28 @@ template <class R, bool CPLX> struct Impl {
       return GPE_OK;
    }
 
+   template <int AXIS, bool NU> static gpe_status sweep_xy(gpe_solver *s, double g, double gd) {
+      const auto &w = s->sw[AXIS];
+      if (w.MSEG == 8) return w.S == 3 ? sweep_xy_launch<AXIS, NU, 8, 3>(s, g, gd) : sweep_xy_launch<AXIS, NU, 8, 2>(s, g, gd);
+      return w.S == 3 ? sweep_xy_launch<AXIS, NU, 16, 3>(s, g, gd) : sweep_xy_launch<AXIS, NU, 16, 2>(s, g, gd);
+   }
+
    // x sweep; with nu the pending 1/norm and calcnu are applied on load
    // (calcnu_kernel imag3d-mpicuda.cu:1759 fused with calclux_kernel :1802).
    static gpe_status xsweep(gpe_solver *s, bool nu, double g, double gd) {
-      if (s->sw[0].MSEG == 8) return nu ? sweep_xy_launch<0, true, 8>(s, g, gd) : sweep_xy_launch<0, false, 8>(s, g, gd);
-      return nu ? sweep_xy_launch<0, true, 16>(s, g, gd) : sweep_xy_launch<0, false, 16>(s, g, gd);
+      return nu ? sweep_xy<0, true>(s, g, gd) : sweep_xy<0, false>(s, g, gd);
    }
 
-   static gpe_status ysweep(gpe_solver *s) {
-      if (s->sw[1].MSEG == 8) return sweep_xy_launch<1, false, 8>(s, 0., 0.);
-      return sweep_xy_launch<1, false, 16>(s, 0., 0.);
-   }
+   static gpe_status ysweep(gpe_solver *s) { return sweep_xy<1, false>(s, 0., 0.); }
 
-   template <bool SIMP, int MSEG> static gpe_status sweep_z_launch(gpe_solver *s) {
+   template <bool SIMP, int MSEG, int S> static gpe_status sweep_z_launch(gpe_solver *s) {
       auto &w = s->sw[2];
       const Dims &d = s->d;
-      const void *f = (const void *) k_sweep_z<R, CPLX, SIMP, MSEG>;
+      const void *f = (const void *) k_sweep_z<R, CPLX, SIMP, MSEG, S>;
       CKS(smem_attr(f, w.smem));
-      k_sweep_z<R, CPLX, SIMP, MSEG><<<blocks_for(d.nxy, w.TW), ((w.TW * w.tab.P + 31) & ~31), w.smem, s->st>>>(
+      const long long ntiles = (d.nxy + w.TW - 1) / w.TW;
+      const unsigned grid = (unsigned) std::min<long long>(ntiles, (long long) w.ctas * s->nsm);
+      k_sweep_z<R, CPLX, SIMP, MSEG, S><<<grid, ((w.TW * w.tab.P + 31) & ~31), w.smem, s->st>>>(
           (P *) s->psi, d, w.tab, w.TW, w.LS, s->wz, s->p.dz / 3., s->rowA, s->err);
       CKL();
       mark(s);
@@ -634,8 +647,13 @@ template <class R, bool CPLX> struct Impl {
 
    // z sweep; with simp each row also yields its Simpson integral of |psi|^2
    static gpe_status zsweep(gpe_solver *s, bool simp) {
-      if (s->sw[2].MSEG == 8) return simp ? sweep_z_launch<true, 8>(s) : sweep_z_launch<false, 8>(s);
-      return simp ? sweep_z_launch<true, 16>(s) : sweep_z_launch<false, 16>(s);
+      const auto &w = s->sw[2];
+      if (w.MSEG == 8) {
+         if (w.S == 3) return simp ? sweep_z_launch<true, 8, 3>(s) : sweep_z_launch<false, 8, 3>(s);
+         return simp ? sweep_z_launch<true, 8, 2>(s) : sweep_z_launch<false, 8, 2>(s);
+      }
+      if (w.S == 3) return simp ? sweep_z_launch<true, 16, 3>(s) : sweep_z_launch<false, 16, 3>(s);
+      return simp ? sweep_z_launch<true, 16, 2>(s) : sweep_z_launch<false, 16, 2>(s);
    }
 
    static gpe_status norm_final(gpe_solver *s, double *dev_out) {

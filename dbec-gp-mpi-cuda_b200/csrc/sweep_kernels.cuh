@@ -203,126 +203,172 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
 }
 
 // ---------------------------------------------------------------------------
+// Persistent pipelined CTAs.  A CTA walks the tiles t = blockIdx.x,
+// blockIdx.x + gridDim.x, ... through S shared-memory stages: while it sweeps
+// tile i, the TMA engine already loads tile i+1 into the next stage and
+// stores tile i-1 from the previous one.  Thread 0 issues every copy; before
+// refilling a stage it waits until the bulk store that last read the stage
+// has finished reading (all but the newest S-2 store groups).
+template <int S> __device__ __forceinline__ void wait_stage_free() {
+   if constexpr (S == 2) bulk_wait_read<0>();
+   else if constexpr (S == 3) bulk_wait_read<1>();
+   else bulk_wait_read<2>();
+}
+
 // x or y sweep.  Tile: TW consecutive z columns of one y (x sweep) or one x
 // (y sweep) plane, the whole line along the swept axis, brought in by TMA.
 // With NU the x sweep first applies the pending 1/norm and calcnu to the tile
 // (needs phi).
-template <class R, bool CPLX, int AXIS, bool NU, int MSEG>
-__global__ void __launch_bounds__(256, 3) k_sweep_xy(const __grid_constant__ CUtensorMap tm_psi,
+template <class R, bool CPLX, int AXIS, bool NU, int MSEG, int S>
+__global__ void __launch_bounds__(256, 2) k_sweep_xy(const __grid_constant__ CUtensorMap tm_psi,
                                                      const __grid_constant__ CUtensorMap tm_phi, Dims d, SegTab tb,
                                                      Trap trap, double g, double gd, double dt,
                                                      const State *__restrict__ st, int TW, int boxn, int nbox,
                                                      uint32_t *err) {
    using P = typename Tr<R, CPLX>::P;
    extern __shared__ __align__(16) unsigned char smem_raw[];
-   __shared__ __align__(8) uint64_t bar;
+   __shared__ __align__(8) uint64_t full[S];
    const int n = tb.n;
    const int rows = boxn * nbox;  // rows staged (>= n)
-   // layout: tile | phi tile | block maps  (TMA targets 128-byte aligned)
-   P *tile = (P *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
-   R *ptile = (R *) (tile + rows * TW);
-   P *blk = (P *) (((uintptr_t) (ptile + (NU ? rows * TW : 0)) + 15) & ~(uintptr_t) 15);
-   const int nzb = (d.nz + TW - 1) / TW;
-   const int other = blockIdx.x / nzb;  // y for the x sweep, x for the y sweep
-   const int z0 = (blockIdx.x - other * nzb) * TW;
    constexpr int E = CPLX ? 2 : 1;
    const uint32_t psi_bytes = (uint32_t) (rows * TW * sizeof(P));
    const uint32_t phi_bytes = NU ? (uint32_t) (rows * TW * sizeof(R)) : 0u;
+   const uint32_t stage_bytes = (psi_bytes + phi_bytes + 127u) & ~127u;
+   // layout: S stages of (tile | phi tile) | block maps  (TMA targets 128-byte aligned)
+   unsigned char *base = (unsigned char *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
+   P *blk = (P *) (base + S * stage_bytes);
+   const int nzb = (d.nz + TW - 1) / TW;
+   const int ntiles = (AXIS == 0 ? d.ny : d.nx) * nzb;
+   auto copy_tile = [&](int t, int q, bool load) {
+      const int other = t / nzb, z0 = (t - other * nzb) * TW;
+      P *tile = (P *) (base + q * stage_bytes);
+      R *ptile = (R *) (tile + rows * TW);
+      if (load) mbar_arrive_expect_tx(&full[q], psi_bytes + phi_bytes);
+      for (int b = 0; b < nbox; b++) {
+         const int a0 = b * boxn;
+         if (load) {
+            if (AXIS == 0) tma_load_3d(tile + a0 * TW, &tm_psi, E * z0, other, a0, &full[q]);
+            else tma_load_3d(tile + a0 * TW, &tm_psi, E * z0, a0, other, &full[q]);
+            if (NU) {
+               if (AXIS == 0) tma_load_3d(ptile + a0 * TW, &tm_phi, z0, other, a0, &full[q]);
+               else tma_load_3d(ptile + a0 * TW, &tm_phi, z0, a0, other, &full[q]);
+            }
+         } else {
+            if (AXIS == 0) tma_store_3d(&tm_psi, E * z0, other, a0, tile + a0 * TW);
+            else tma_store_3d(&tm_psi, E * z0, a0, other, tile + a0 * TW);
+         }
+      }
+      if (!load) bulk_commit();
+   };
    if (threadIdx.x == 0) {
-      mbar_init(&bar, 1);
+      for (int q = 0; q < S; q++) mbar_init(&full[q], 1);
       fence_mbar_init();
    }
    __syncthreads();
-   if (threadIdx.x == 0) {
-      mbar_arrive_expect_tx(&bar, psi_bytes + phi_bytes);
-      for (int b = 0; b < nbox; b++) {
-         const int a0 = b * boxn;
-         if (AXIS == 0) tma_load_3d(tile + a0 * TW, &tm_psi, E * z0, other, a0, &bar);
-         else tma_load_3d(tile + a0 * TW, &tm_psi, E * z0, a0, other, &bar);
-         if (NU) {
-            if (AXIS == 0) tma_load_3d(ptile + a0 * TW, &tm_phi, z0, other, a0, &bar);
-            else tma_load_3d(ptile + a0 * TW, &tm_phi, z0, a0, other, &bar);
-         }
-      }
-   }
-   // a timed-out copy makes the whole CTA leave together
-   if (__syncthreads_or(!mbar_wait(&bar, 0, err))) return;
-   if (NU) {
-      const double scale = st->scale;
-      const R invN = (R) (1.0 / (double) d.npts);
-      for (int e = threadIdx.x; e < n * TW; e += blockDim.x) {
-         const int i = e / TW, cc = e - i * TW;
-         const int k = z0 + cc;
-         if (k < d.nz) {
-            const R V = (R) (AXIS == 0 ? trap.v(i, other, k) : trap.v(other, i, k));
-            tile[e] = nu_op<R>(scl(tile[e], scale), ptile[e], V, (R) g, (R) gd, (R) dt, invN);
-         }
-      }
-      __syncthreads();
-   }
+   if (threadIdx.x == 0 && (int) blockIdx.x < ntiles) copy_tile(blockIdx.x, 0, true);
+   const double scale = NU ? st->scale : 1.;
+   const R invN = (R) (1.0 / (double) d.npts);
    const int c = threadIdx.x % TW, p = threadIdx.x / TW;
-   seg_sweep<R, CPLX, MSEG>(tile, TW, 1, c, p, TW, tb, blk, nullptr, nullptr);
-   fence_proxy_async();
-   __syncthreads();
-   if (threadIdx.x == 0) {
-      for (int b = 0; b < nbox; b++) {
-         const int a0 = b * boxn;
-         if (AXIS == 0) tma_store_3d(&tm_psi, E * z0, other, a0, tile + a0 * TW);
-         else tma_store_3d(&tm_psi, E * z0, a0, other, tile + a0 * TW);
+   int i = 0;
+   for (int t = blockIdx.x; t < ntiles; t += gridDim.x, i++) {
+      const int q = i % S;
+      if (threadIdx.x == 0 && t + (int) gridDim.x < ntiles) {
+         wait_stage_free<S>();
+         copy_tile(t + gridDim.x, (i + 1) % S, true);
       }
-      bulk_commit();
-      bulk_wait_all();
+      // a timed-out copy makes the whole CTA leave together
+      if (__syncthreads_or(!mbar_wait(&full[q], (i / S) & 1, err))) break;
+      P *tile = (P *) (base + q * stage_bytes);
+      if (NU) {
+         const int other = t / nzb, z0 = (t - other * nzb) * TW;
+         const R *ptile = (const R *) (tile + rows * TW);
+         for (int e = threadIdx.x; e < n * TW; e += blockDim.x) {
+            const int ii = e / TW, cc = e - ii * TW;
+            const int k = z0 + cc;
+            if (k < d.nz) {
+               const R V = (R) (AXIS == 0 ? trap.v(ii, other, k) : trap.v(other, ii, k));
+               tile[e] = nu_op<R>(scl(tile[e], scale), ptile[e], V, (R) g, (R) gd, (R) dt, invN);
+            }
+         }
+         __syncthreads();
+      }
+      seg_sweep<R, CPLX, MSEG>(tile, TW, 1, c, p, TW, tb, blk, nullptr, nullptr);
+      fence_proxy_async();
+      __syncthreads();
+      if (threadIdx.x == 0) copy_tile(t, q, false);
    }
+   if (threadIdx.x == 0) bulk_wait_all();
 }
 
 // z sweep.  Tile: TR consecutive (x, y) rows, each copied by one bulk copy to
 // a padded shared row (stride LS elements).  With SIMP every row also yields
 // its Simpson integral of |psi'|^2 (simpint over z, diffint.cu:106) for the
 // norm of the step.
-template <class R, bool CPLX, bool SIMP, int MSEG>
-__global__ void __launch_bounds__(256, 3) k_sweep_z(typename Tr<R, CPLX>::P *__restrict__ psi, Dims d, SegTab tb,
+template <class R, bool CPLX, bool SIMP, int MSEG, int S>
+__global__ void __launch_bounds__(256, 2) k_sweep_z(typename Tr<R, CPLX>::P *__restrict__ psi, Dims d, SegTab tb,
                                                     int TR, int LS, const double *__restrict__ wz, double hz3,
                                                     double *__restrict__ rowsum, uint32_t *err) {
    using P = typename Tr<R, CPLX>::P;
    extern __shared__ __align__(16) unsigned char smem_raw[];
-   __shared__ __align__(8) uint64_t bar;
-   // layout: rows (stride LS) | block maps | Simpson partials
-   P *tile = (P *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
-   const int NW = (tb.P + 32 / TR - 1) / (32 / TR);
-   P *blk = tile + TR * LS;
-   double *part = (double *) (blk + 2 * (NW + 1) * TR);
+   __shared__ __align__(8) uint64_t full[S];
    const int nz = d.nz;
-   const long long r0 = (long long) blockIdx.x * TR;
-   const int nr = (int) ((d.nxy - r0) < TR ? (d.nxy - r0) : TR);
    const uint32_t row_bytes = (uint32_t) (nz * sizeof(P));
+   const uint32_t stage_bytes = ((uint32_t) (TR * LS * sizeof(P)) + 127u) & ~127u;
+   // layout: S stages of rows | block maps | Simpson partials
+   unsigned char *base = (unsigned char *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
+   const int NW = (tb.P + 32 / TR - 1) / (32 / TR);
+   P *blk = (P *) (base + S * stage_bytes);
+   double *part = (double *) (blk + 2 * (NW + 1) * TR);
+   const int ntiles = (int) ((d.nxy + TR - 1) / TR);
+   auto nrows = [&](int t) -> int {
+      const long long r0 = (long long) t * TR;
+      return (int) ((d.nxy - r0) < TR ? (d.nxy - r0) : TR);
+   };
+   auto copy_tile = [&](int t, int q, bool load) {
+      P *tile = (P *) (base + q * stage_bytes);
+      const int nr = nrows(t);
+      if (load) mbar_arrive_expect_tx(&full[q], row_bytes * nr);
+      for (int r = 0; r < nr; r++) {
+         P *g = psi + ((long long) t * TR + r) * nz;
+         if (load) bulk_load(tile + r * LS, g, row_bytes, &full[q]);
+         else bulk_store(g, tile + r * LS, row_bytes);
+      }
+      if (!load) bulk_commit();
+   };
    if (threadIdx.x == 0) {
-      mbar_init(&bar, 1);
+      for (int q = 0; q < S; q++) mbar_init(&full[q], 1);
       fence_mbar_init();
    }
    __syncthreads();
-   if (threadIdx.x == 0) {
-      mbar_arrive_expect_tx(&bar, row_bytes * nr);
-      for (int r = 0; r < nr; r++) bulk_load(tile + r * LS, psi + (r0 + r) * nz, row_bytes, &bar);
-   }
-   // rows beyond the grid (last tile) are zero so their sweep stays finite
-   for (int e = threadIdx.x; e < (TR - nr) * LS; e += blockDim.x) tile[nr * LS + e] = zero_of<P>();
-   if (__syncthreads_or(!mbar_wait(&bar, 0, err))) return;
+   if (threadIdx.x == 0 && (int) blockIdx.x < ntiles) copy_tile(blockIdx.x, 0, true);
    const int c = threadIdx.x % TR, p = threadIdx.x / TR;
-   double my = 0.;
-   seg_sweep<R, CPLX, MSEG>(tile, 1, LS, c, p, TR, tb, blk, SIMP ? wz : nullptr, SIMP ? &my : nullptr);
-   if (SIMP && p < tb.P) part[p * TR + c] = my;
-   fence_proxy_async();
-   __syncthreads();
-   if (SIMP && p == 0 && c < nr) {
-      double sum = 0.;
-      for (int pp = 0; pp < tb.P; pp++) sum += part[pp * TR + c];
-      rowsum[r0 + c] = sum * hz3;
+   int i = 0;
+   for (int t = blockIdx.x; t < ntiles; t += gridDim.x, i++) {
+      const int q = i % S;
+      if (threadIdx.x == 0 && t + (int) gridDim.x < ntiles) {
+         wait_stage_free<S>();
+         copy_tile(t + gridDim.x, (i + 1) % S, true);
+      }
+      if (__syncthreads_or(!mbar_wait(&full[q], (i / S) & 1, err))) break;
+      P *tile = (P *) (base + q * stage_bytes);
+      const int nr = nrows(t);
+      if (nr < TR) {  // rows beyond the grid are zero so their sweep stays finite
+         for (int e = threadIdx.x; e < (TR - nr) * LS; e += blockDim.x) tile[nr * LS + e] = zero_of<P>();
+         __syncthreads();
+      }
+      double my = 0.;
+      seg_sweep<R, CPLX, MSEG>(tile, 1, LS, c, p, TR, tb, blk, SIMP ? wz : nullptr, SIMP ? &my : nullptr);
+      if (SIMP && p < tb.P) part[p * TR + c] = my;
+      fence_proxy_async();
+      __syncthreads();
+      if (SIMP && p == 0 && c < nr) {
+         double sum = 0.;
+         for (int pp = 0; pp < tb.P; pp++) sum += part[pp * TR + c];
+         rowsum[(long long) t * TR + c] = sum * hz3;
+      }
+      if (threadIdx.x == 0) copy_tile(t, q, false);
    }
-   if (threadIdx.x == 0) {
-      for (int r = 0; r < nr; r++) bulk_store(psi + (r0 + r) * nz, tile + r * LS, row_bytes);
-      bulk_commit();
-      bulk_wait_all();
-   }
+   if (threadIdx.x == 0) bulk_wait_all();
 }
 
 }  // namespace gpe

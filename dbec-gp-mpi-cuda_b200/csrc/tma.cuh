@@ -109,5 +109,10 @@ __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.comm
 __device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
 // all committed bulk stores of this thread are complete
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+// all but the newest N committed bulk-store groups have finished reading
+// shared memory (N = pipeline stages - 2, an immediate)
+template <int N> __device__ __forceinline__ void bulk_wait_read() {
+   asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
 
 }  // namespace gpe
