@@ -14,6 +14,8 @@ namespace gpe {
 
 struct Dims {
    int nx, ny, nz, nzh;
+   int nzp;  // row pitch of the half spectrum in complex elements: nzh, or
+             // nzh rounded up to even for complex64 so rows stay 16-byte multiples
    long long nxy, npts;
 };
 

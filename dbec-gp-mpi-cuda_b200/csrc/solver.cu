@@ -152,7 +152,8 @@ extern "C" gpe_status gpe_device_bytes(const gpe_params *p, long long *bytes) {
    const size_t r = (p->precision == GPE_PREC_MIXED) ? 4 : 8;
    long long b = 0;
    b += npts * (long long) psi_esz(p);                   // psi
-   b += nzh * p->nx * p->ny * (long long) (2 * r);       // spectrum
+   const long long nzp = (p->precision == GPE_PREC_MIXED) ? (nzh + 1) & ~1LL : nzh;
+   b += nzp * p->nx * p->ny * (long long) (2 * r);       // spectrum (rows padded to 16 bytes)
    b += npts * (long long) r;                            // phi
    b += nzh * (p->nx / 2 + 1) * (p->ny / 2 + 1) * 8;     // Udd octant
    b += 4 * std::max(p->nx * p->ny, std::max(p->nx * p->nz, p->ny * p->nz)) * 8;  // row sums
@@ -304,11 +305,14 @@ static gpe_status encoder(EncodeTiledFn *fn) {
 
 // 3D tensor map over a [nx][ny][w * nz] array of `esz`-byte scalars with box
 // {bw, by, bx} (innermost first).
-static gpe_status make_tmap(CUtensorMap *m, void *base, size_t esz, long w_nz, long ny, long nx, int bw, int by, int bx) {
+// Rows are `pitch` elements apart (pitch = w_nz when 0).
+static gpe_status make_tmap(CUtensorMap *m, void *base, size_t esz, long w_nz, long ny, long nx, int bw, int by, int bx,
+                            long pitch = 0) {
    EncodeTiledFn enc;
    CKS(encoder(&enc));
+   if (pitch == 0) pitch = w_nz;
    cuuint64_t dims[3] = {(cuuint64_t) w_nz, (cuuint64_t) ny, (cuuint64_t) nx};
-   cuuint64_t strides[2] = {(cuuint64_t) (w_nz * esz), (cuuint64_t) (w_nz * esz * ny)};
+   cuuint64_t strides[2] = {(cuuint64_t) (pitch * esz), (cuuint64_t) (pitch * esz * ny)};
    cuuint32_t box[3] = {(cuuint32_t) bw, (cuuint32_t) by, (cuuint32_t) bx};
    cuuint32_t es[3] = {1, 1, 1};
    CUresult r = enc(m, esz == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims,
@@ -376,8 +380,8 @@ static gpe_status setup_sweeps(gpe_solver *s) {
       s->nboxy = (d.ny + s->boxy - 1) / s->boxy;
       s->boxx = (int) std::min<long>(d.nx, 256);
       s->nboxx = (d.nx + s->boxx - 1) / s->boxx;
-      CKS(make_tmap(&s->tm_spec_y, s->spec, rsz, 2 * d.nzh, d.ny, d.nx, 2 * L, s->boxy, 1));
-      CKS(make_tmap(&s->tm_spec_x, s->spec, rsz, 2 * d.nzh, d.ny, d.nx, 2 * L, 1, s->boxx));
+      CKS(make_tmap(&s->tm_spec_y, s->spec, rsz, 2 * d.nzh, d.ny, d.nx, 2 * L, s->boxy, 1, 2 * d.nzp));
+      CKS(make_tmap(&s->tm_spec_x, s->spec, rsz, 2 * d.nzh, d.ny, d.nx, 2 * L, 1, s->boxx, 2 * d.nzp));
    }
    // Simpson weights along z: sum_k wz[k] f[k] * dz / 3 equals simpint (diffint.cu:37-66)
    std::vector<double> wz(d.nz, 0.);
@@ -453,6 +457,7 @@ static gpe_status create_impl(const gpe_params *p, void *stream, gpe_solver *s) 
    }
    Dims &d = s->d;
    d.nx = (int) p->nx; d.ny = (int) p->ny; d.nz = (int) p->nz; d.nzh = d.nz / 2 + 1;
+   d.nzp = s->fp32 ? (d.nzh + 1) & ~1 : d.nzh;
    d.nxy = (long long) d.nx * d.ny;
    d.npts = d.nxy * d.nz;
    make_plan(d.nx, s->px);
@@ -466,7 +471,7 @@ static gpe_status create_impl(const gpe_params *p, void *stream, gpe_solver *s) 
    s->LSo = (int) (d.nz + 16 / s->esz_r);
 
    CK(cudaMalloc(&s->psi, s->esz_psi * d.npts));
-   CK(cudaMalloc(&s->spec, s->esz_c * (size_t) d.nzh * d.nxy));
+   CK(cudaMalloc(&s->spec, s->esz_c * (size_t) d.nzp * d.nxy));
    CK(cudaMalloc(&s->phi, r * d.npts));
    CK(cudaMemset(s->psi, 0, s->esz_psi * d.npts));
    s->row_cap = std::max(d.nxy, std::max((long long) d.nx * d.nz, (long long) d.ny * d.nz));
@@ -586,7 +591,7 @@ template <class R, bool CPLX> struct Impl {
       CKL();
       mark(s);
       {
-         const size_t in_el = std::max((size_t) L * d.nzh, ((size_t) L * s->LSo * sizeof(R) + sizeof(C) - 1) / sizeof(C));
+         const size_t in_el = std::max((size_t) L * d.nzp, ((size_t) L * s->LSo * sizeof(R) + sizeof(C) - 1) / sizeof(C));
          const size_t sm = 128 + ((in_el + 7) & ~(size_t) 7) * sizeof(C) + 2 * (size_t) h * L * sizeof(C) + d.nz * sizeof(C);
          CKS(smem_attr((const void *) k_zinv<R>, sm));
          k_zinv<R><<<grows, 256, sm, s->st>>>(spec, (R *) s->phi, d, s->ph, (const C *) s->twz, s->LSo, s->err);

@@ -23,6 +23,39 @@ namespace gpe {
 
 template <class R> struct FftL { static constexpr int L = 128 / (2 * (int) sizeof(R)); };
 
+// |psi|^2 of L rows (row stride LS elements) packed as complex lines of
+// length h = nz/2 in the interleaved layout: buf[m L + l] = (rho[2m], rho[2m+1]).
+template <class R, bool CPLX, int L>
+__device__ __forceinline__ void zfwd_pack(const typename Tr<R, CPLX>::P *rows, int LS, cpx<R> *buf, int h) {
+   for (int e = threadIdx.x; e < h * L; e += blockDim.x) {
+      const int l = e % L, m = e / L;
+      const typename Tr<R, CPLX>::P *rw = rows + l * LS + 2 * m;
+      buf[e] = mk<R>(dens2(rw[0]), dens2(rw[1]));
+   }
+}
+
+// Real-FFT split of the transformed lines Z into half-spectrum rows
+// out[l pitch + k], k < nzh, zero padding for nzh <= k < nzp, rows l < nr.
+template <class R, int L>
+__device__ __forceinline__ void zfwd_split(const cpx<R> *Z, const cpx<R> *tw, int h, int nzh, int nzp,
+                                           cpx<R> *out, long long pitch, int nr) {
+   using C = cpx<R>;
+   for (int e = threadIdx.x; e < nzp * L; e += blockDim.x) {
+      const int l = e % L, k = e / L;
+      if (l >= nr) continue;
+      if (k >= nzh) {  // row padding
+         out[l * pitch + k] = mk<R>(0, 0);
+         continue;
+      }
+      const C a = Z[(k == h ? 0 : k) * L + l];
+      const C b = cconj(Z[(k == 0 ? 0 : h - k) * L + l]);
+      const C E = cscale(cadd(a, b), (R) 0.5);
+      const C t = csub(a, b);
+      const C O = mk<R>(t.y * (R) 0.5, -t.x * (R) 0.5);
+      out[l * pitch + k] = cadd(E, cmul(tw[k], O));
+   }
+}
+
 // Pass 1: |psi|^2 rows -> half spectrum rows (L rows per CTA).
 template <class R, bool CPLX>
 __global__ void __launch_bounds__(256) k_zfwd(const typename Tr<R, CPLX>::P *__restrict__ psi,
@@ -33,8 +66,8 @@ __global__ void __launch_bounds__(256) k_zfwd(const typename Tr<R, CPLX>::P *__r
    constexpr int L = FftL<R>::L;
    extern __shared__ __align__(16) unsigned char smem_raw[];
    __shared__ __align__(8) uint64_t bar;
-   const int nz = d.nz, h = nz / 2, nzh = d.nzh;
-   // layout: rows [L][LSr] (later the output rows [L][nzh]) | bufA | bufB | twiddles
+   const int nz = d.nz, h = nz / 2, nzh = d.nzh, nzp = d.nzp;
+   // layout: rows [L][LSr] (later the output rows [L][nzp]) | bufA | bufB | twiddles
    P *rows = (P *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
    C *bufA = (C *) (rows + L * LSr);
    C *bufB = bufA + h * L;
@@ -54,27 +87,15 @@ __global__ void __launch_bounds__(256) k_zfwd(const typename Tr<R, CPLX>::P *__r
    }
    for (int e = threadIdx.x; e < (L - nr) * LSr; e += blockDim.x) rows[nr * LSr + e] = zero_of<P>();
    if (__syncthreads_or(!mbar_wait(&bar, 0, err))) return;
-   for (int e = threadIdx.x; e < h * L; e += blockDim.x) {
-      const int l = e % L, m = e / L;
-      const P *rw = rows + l * LSr + 2 * m;
-      bufA[e] = mk<R>(dens2(rw[0]), dens2(rw[1]));
-   }
+   zfwd_pack<R, CPLX, L>(rows, LSr, bufA, h);
    __syncthreads();
    const C *Z = fft_lines<L, C, false>(bufA, bufB, ph, tw, 2);
-   C *out = (C *) rows;  // [L][nzh]; the rows are no longer read
-   for (int e = threadIdx.x; e < nzh * L; e += blockDim.x) {
-      const int l = e % L, k = e / L;
-      const C a = Z[(k == h ? 0 : k) * L + l];
-      const C b = cconj(Z[(k == 0 ? 0 : h - k) * L + l]);
-      const C E = cscale(cadd(a, b), (R) 0.5);
-      const C t = csub(a, b);
-      const C O = mk<R>(t.y * (R) 0.5, -t.x * (R) 0.5);
-      out[l * nzh + k] = cadd(E, cmul(tw[k], O));
-   }
+   C *out = (C *) rows;  // [L][nzp]; the rows are no longer read
+   zfwd_split<R, L>(Z, tw, h, nzh, nzp, out, nzp, L);
    fence_proxy_async();
    __syncthreads();
    if (threadIdx.x == 0) {
-      bulk_store(spec + r0 * nzh, out, (uint32_t) (nr * nzh * sizeof(C)));
+      bulk_store(spec + r0 * nzp, out, (uint32_t) (nr * nzp * sizeof(C)));
       bulk_commit();
       bulk_wait_all();
    }
@@ -173,10 +194,10 @@ __global__ void __launch_bounds__(256) k_zinv(const cpx<R> *__restrict__ spec, R
    constexpr int L = FftL<R>::L;
    extern __shared__ __align__(16) unsigned char smem_raw[];
    __shared__ __align__(8) uint64_t bar;
-   const int nz = d.nz, h = nz / 2, nzh = d.nzh;
-   // layout: input rows [L][nzh] (later the phi rows [L][LSo]) | bufA | bufB | twiddles
+   const int nz = d.nz, h = nz / 2, nzp = d.nzp;
+   // layout: input rows [L][nzp] (later the phi rows [L][LSo]) | bufA | bufB | twiddles
    C *in = (C *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
-   const int in_elems = ((L * nzh) > (L * LSo + 1) / 2 ? (L * nzh) : (L * LSo + 1) / 2);
+   const int in_elems = ((L * nzp) > (L * LSo + 1) / 2 ? (L * nzp) : (L * LSo + 1) / 2);
    C *bufA = in + ((in_elems + 7) & ~7);
    C *bufB = bufA + h * L;
    C *tw = bufB + h * L;
@@ -188,16 +209,16 @@ __global__ void __launch_bounds__(256) k_zinv(const cpx<R> *__restrict__ spec, R
    }
    __syncthreads();
    if (threadIdx.x == 0) {
-      mbar_arrive_expect_tx(&bar, (uint32_t) (nr * nzh * sizeof(C) + nz * sizeof(C)));
+      mbar_arrive_expect_tx(&bar, (uint32_t) (nr * nzp * sizeof(C) + nz * sizeof(C)));
       bulk_load(tw, twz, (uint32_t) (nz * sizeof(C)), &bar);
-      bulk_load(in, spec + r0 * nzh, (uint32_t) (nr * nzh * sizeof(C)), &bar);
+      bulk_load(in, spec + r0 * nzp, (uint32_t) (nr * nzp * sizeof(C)), &bar);
    }
-   for (int e = threadIdx.x; e < (L - nr) * nzh; e += blockDim.x) in[nr * nzh + e] = mk<R>(0, 0);
+   for (int e = threadIdx.x; e < (L - nr) * nzp; e += blockDim.x) in[nr * nzp + e] = mk<R>(0, 0);
    if (__syncthreads_or(!mbar_wait(&bar, 0, err))) return;
    for (int e = threadIdx.x; e < h * L; e += blockDim.x) {
       const int l = e % L, k = e / L;
-      C a = in[l * nzh + k];
-      C b = in[l * nzh + h - k];
+      C a = in[l * nzp + k];
+      C b = in[l * nzp + h - k];
       if (k == 0) { a.y = 0; b.y = 0; }  // DC and Nyquist bins are real
       b = cconj(b);
       const C E = cadd(a, b);

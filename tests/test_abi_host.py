@@ -30,7 +30,8 @@ def test_library_exports_every_declared_symbol(gpe_lib):
 
 
 @pytest.mark.parametrize("bad", [dict(nx=7), dict(nx=14), dict(ny=2), dict(nz=2048), dict(dt=0.0), dict(cutoff=-1.0),
-                                 dict(mode=3), dict(precision=5)])
+                                 dict(mode=3), dict(precision=5),
+                                 dict(precision=1, nz=18)])
 def test_invalid_parameters_rejected_without_gpu(gpe_lib, bad):
     kw = dict(mode=0, nx=16, ny=16, nz=16, dx=.2, dy=.2, dz=.2, dt=.001, gamma=1., nu=1., lamda=1., cutoff=1.)
     kw.update(bad)

@@ -1,0 +1,115 @@
+"""Mixed-precision path against the FP64 oracle.
+
+The mixed handle keeps psi, the spectrum and phi in FP32 / complex64 and runs
+the FFT passes, the sweeps and the exponentials in FP32, while the norm
+reduction, the renormalisation factor, the mu / E / rms accumulators, the
+Thomas alpha / gamma tables and U_dd(k) stay FP64.  Each test runs the same
+initial psi through the oracle (FP64) and states the error it allows:
+
+* imaginary-time ground state (64^3, 1000 renormalised steps):
+  |dmu/mu| <= 1e-6, |dE/E| <= 1e-6, rms sizes and the norm <= 1e-6 relative,
+  density L2 (||rho - rho_ref||_2 / ||rho_ref||_2) <= 1e-5;
+* real-time evolution (200 complex64 steps): the same bars on mu, E, rms,
+  norm and density;
+* single operators: <= 2e-6 relative (max-abs error over max-abs value),
+  a few FP32 roundings of the largest value.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+MIX_OP_TOL = 2e-6
+MIX_OBS_TOL = 1e-6
+MIX_DENS_TOL = 1e-5
+
+
+def rel(a, b):
+    return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / max(np.max(np.abs(np.asarray(b))), 1e-300))
+
+
+def dens_l2(a, b):
+    ra, rb = np.abs(a) ** 2, np.abs(b) ** 2
+    return float(np.linalg.norm((ra - rb).ravel()) / np.linalg.norm(rb.ravel()))
+
+
+def make_pair(gpe, orc, mode, shape, spacing=(.25, .25, .25), dt=.00625, trap=(.5, 1., 1.5), opt=1):
+    nx, ny, nz = shape
+    cutoff = 0.5 * min(nx * spacing[0], ny * spacing[1], nz * spacing[2])
+    p = gpe.make_params(mode, nx, ny, nz, *spacing, dt, *trap, cutoff, opt=opt, precision=gpe.PREC_MIXED)
+    s = gpe.Solver(p)
+    o = orc.Oracle(mode, opt, nx, ny, nz, *spacing, dt, *trap, cutoff)
+    return s, o
+
+
+def seeded_psi(shape, mode, seed=3):
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = shape
+    x = np.linspace(-1, 1, nx)[:, None, None]
+    y = np.linspace(-1, 1, ny)[None, :, None]
+    z = np.linspace(-1, 1, nz)[None, None, :]
+    psi = np.exp(-3 * (x * x + 1.5 * y * y + 2 * z * z)) * (1 + 0.1 * rng.standard_normal(shape))
+    if mode == 1:
+        psi = psi * np.exp(1j * (0.3 * x + 0.2 * y * z))
+        # values an FP32 psi holds exactly, so both sides start from the same state
+        return psi.real.astype(np.float32).astype(np.float64) + 1j * psi.imag.astype(np.float32).astype(np.float64)
+    return psi.astype(np.float32).astype(np.float64)
+
+
+def _observables_close(s, o, g, gd, tol):
+    mu_s, en_s = s.calcmuen(g, gd)
+    mu_o, en_o = o.calcmuen(g, gd)
+    errs = dict(mu=abs(mu_s / mu_o - 1), en=abs(en_s / en_o - 1), rms=rel(s.calcrms(), o.calcrms()),
+                norm=abs(s.calcnorm(False) / o.calcnorm(False) - 1))
+    for k, v in errs.items():
+        assert v <= tol, (k, errs)
+    return errs
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_mixed_operators_match_oracle(gpe_lib, oracle_mod, mode):
+    shape = (24, 20, 32)
+    s, o = make_pair(gpe_lib, oracle_mod, mode, shape)
+    psi = seeded_psi(shape, mode)
+    s.set_psi(psi)
+    o.set_psi(psi)
+    s.calcpsidd2()
+    o.calcpsidd2()
+    assert rel(s.get_phi(), o.get_phi()) <= MIX_OP_TOL
+    s.calcnu(37.0, 11.0)
+    o.calcnu(37.0, 11.0)
+    assert rel(s.get_psi(), o.get_psi()) <= MIX_OP_TOL
+    for name in ("calclux", "calcluy", "calcluz"):
+        getattr(s, name)()
+        getattr(o, name)()
+        assert rel(s.get_psi(), o.get_psi()) <= MIX_OP_TOL, name
+    _observables_close(s, o, 37.0, 11.0, MIX_OP_TOL)
+    s.close()
+
+
+def test_mixed_imag_ground_state_64cube(gpe_lib, oracle_mod):
+    """64^3, dx = 0.25, dt = 0.1 dx^2, trap (0.5, 1, 1.5), g = 100, gd = 30,
+    R = 8, reference Gaussian start, 1000 renormalised steps."""
+    s, o = make_pair(gpe_lib, oracle_mod, 0, (64, 64, 64))
+    s.init_gaussian()
+    o.init_gaussian()
+    s.calcnorm(True)
+    o.calcnorm(True)
+    s.run(1000, 100., 30.)
+    o.run(1000, 100., 30.)
+    _observables_close(s, o, 100., 30., MIX_OBS_TOL)
+    assert dens_l2(s.get_psi(), o.get_psi()) <= MIX_DENS_TOL
+    s.close()
+
+
+def test_mixed_real_time(gpe_lib, oracle_mod):
+    shape = (32, 30, 40)
+    s, o = make_pair(gpe_lib, oracle_mod, 1, shape, dt=.0005)
+    psi = seeded_psi(shape, 1, seed=9)
+    s.set_psi(psi)
+    o.set_psi(psi)
+    s.run(200, 50., 20.)
+    o.run(200, 50., 20.)
+    _observables_close(s, o, 50., 20., MIX_OBS_TOL)
+    assert dens_l2(s.get_psi(), o.get_psi()) <= MIX_DENS_TOL
+    s.close()
