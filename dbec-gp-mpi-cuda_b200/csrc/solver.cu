@@ -366,12 +366,16 @@ static gpe_status setup_sweeps(gpe_solver *s) {
          stage = ((size_t) w.TW * w.LS * esz + 127) & ~(size_t) 127;
          fixed = 128 + blk + (size_t) P * w.TW * sizeof(double);
       }
-      // pipeline depth: 3 stages when two CTAs still fit on an SM, else 2
+      // as many resident CTAs as the kernels are compiled for and shared
+      // memory allows, then the deepest pipeline (2 or 3 stages) that keeps them
       const size_t sm_cap = 227 * 1024;
-      w.S = (fixed + 3 * stage) * 2 <= sm_cap ? 3 : 2;
+      const int max_ctas = kSweepCtas[ax == 0 ? 1 : 0];
+      w.ctas = 0;
+      for (int ct = max_ctas; ct >= 1 && !w.ctas; ct--)
+         for (int S = 3; S >= 2 && !w.ctas; S--)
+            if ((fixed + S * stage) * ct <= sm_cap) { w.ctas = ct; w.S = S; }
+      if (!w.ctas) return fail(GPE_ERR_PARAM, "grid too large for the sweep tiles (shared memory)");
       w.smem = fixed + w.S * stage;
-      if (w.smem > sm_cap) return fail(GPE_ERR_PARAM, "grid too large for the sweep tiles (shared memory)");
-      w.ctas = std::max<int>(1, std::min<int>(2, (int) (sm_cap / w.smem)));
    }
    // spectrum tiles: spec[x][y][kz] viewed as [nx][ny][2 nzh] scalars
    {

@@ -137,9 +137,10 @@ __global__ void __launch_bounds__(256) k_yfft(const __grid_constant__ CUtensorMa
 }
 
 // Pass 3: FFT along x, multiply by Udd(k) * scale^2, inverse FFT along x, for
-// L kz columns of one y plane.  Udd octant layout [|kx|][|ky|][kz].
+// L kz columns of one y plane.  Udd octant layout [|kx|][|ky|][kz].  Compiled
+// for three resident CTAs per SM (their shared tiles fit at nx = 256).
 template <class R>
-__global__ void __launch_bounds__(256) k_xconv(const __grid_constant__ CUtensorMap tm, Dims d, FftPlan px,
+__global__ void __launch_bounds__(256, 3) k_xconv(const __grid_constant__ CUtensorMap tm, Dims d, FftPlan px,
                                                const cpx<R> *__restrict__ twx, const double *__restrict__ udd,
                                                const State *__restrict__ st, int boxn, int nbox, uint32_t *err) {
    using C = cpx<R>;

@@ -49,6 +49,27 @@ template <class R, bool CPLX> struct SegOps {
       if constexpr (CPLX) return cmul(a, b);
       else return a * b;
    }
+   // One backward Thomas step of the Crank-Nicolson system.  With the
+   // coefficients of gencoef, minusA = -A and A0r = 1 + 2A in both modes
+   // (imag: A = -c/2 real; real: A = -i c/2), so the right-hand side
+   //    r = minusA psi[i+1] + A0r psi[i] - A psi[i-1] = psi[i] + A t,
+   //    t = 2 psi[i] - psi[i+1] - psi[i-1],
+   // and gamma (A beta - r) = gamma (A (beta - t) - psi[i]).  `a` is A's
+   // real (imag mode) or imaginary (real mode) part.
+   __device__ static P back_step(P b, P w2, P w1, P w0, P g, R a) {
+      if constexpr (CPLX) {
+         const R tx = fma((R) 2, w1.x, -w2.x) - w0.x, ty = fma((R) 2, w1.y, -w2.y) - w0.y;
+         const R dx = b.x - tx, dy = b.y - ty;
+         const R ux = fma(-a, dy, -w1.x), uy = fma(a, dx, -w1.y);
+         P r;
+         r.x = fma(g.x, ux, -g.y * uy);
+         r.y = fma(g.x, uy, g.y * ux);
+         return r;
+      } else {
+         const R t = fma((R) 2, w1, -w2) - w0;
+         return g * fma(a, b - t, -w1);
+      }
+   }
    __device__ static P fma_(P a, P b, P c) {  // a * b + c
       if constexpr (CPLX) {
          P r;
@@ -92,7 +113,7 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
    const bool top = (p == NP - 1);
    const int hf = top ? n - 3 : lo + m - 1;  // last owned recurrence index
    const int K = hf - lo + 1;                // owned points, 1 <= K <= MSEG
-   const P A = Op::cv(tb.A), A0r = Op::cv(tb.A0r), mA = Op::cv(tb.mA);
+   const R a = CPLX ? (R) tb.A.y : (R) tb.A.x;
    P *line = s + c * cs;
    auto L = [&](int i) -> P { return line[i * es]; };
    P *ba = blk, *bb = blk + (NW + 1) * TW;  // per-warp block maps [NW][TW]
@@ -109,10 +130,7 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
       for (int q = MSEG - 1; q >= 0; q--) {
          if (q < K) {
             const P w0 = L(lo + q);
-            P cc = Op::mul(mA, w2);
-            cc = cadd_any(cc, Op::mul(A0r, w1));
-            cc = csub_any(cc, Op::mul(A, w0));
-            b = Op::mul(Op::ld(tb.ga, lo + q + 1), csub_any(Op::mul(A, b), cc));
+            b = Op::back_step(b, w2, w1, w0, Op::ld(tb.ga, lo + q + 1), a);
             bt[q] = b;
             w2 = w1;
             w1 = w0;
@@ -209,6 +227,12 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
 // stores tile i-1 from the previous one.  Thread 0 issues every copy; before
 // refilling a stage it waits until the bulk store that last read the stage
 // has finished reading (all but the newest S-2 store groups).
+// Resident CTAs per SM the sweep kernels are compiled for (register
+// budget): [0] plain sweeps, [1] the x sweep fused with calcnu, whose tile
+// also stages phi.  The host never launches more per SM.  Three CTAs (80
+// registers) spill the 16-point segments and measured slower on B200.
+constexpr int kSweepCtas[2] = {2, 2};
+
 template <int S> __device__ __forceinline__ void wait_stage_free() {
    if constexpr (S == 2) bulk_wait_read<0>();
    else if constexpr (S == 3) bulk_wait_read<1>();
@@ -220,7 +244,7 @@ template <int S> __device__ __forceinline__ void wait_stage_free() {
 // With NU the x sweep first applies the pending 1/norm and calcnu to the tile
 // (needs phi).
 template <class R, bool CPLX, int AXIS, bool NU, int MSEG, int S>
-__global__ void __launch_bounds__(256, 2) k_sweep_xy(const __grid_constant__ CUtensorMap tm_psi,
+__global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) k_sweep_xy(const __grid_constant__ CUtensorMap tm_psi,
                                                      const __grid_constant__ CUtensorMap tm_phi, Dims d, SegTab tb,
                                                      Trap trap, double g, double gd, double dt,
                                                      const State *__restrict__ st, int TW, int boxn, int nbox,
@@ -268,7 +292,8 @@ __global__ void __launch_bounds__(256, 2) k_sweep_xy(const __grid_constant__ CUt
    if (threadIdx.x == 0 && (int) blockIdx.x < ntiles) copy_tile(blockIdx.x, 0, true);
    const double scale = NU ? st->scale : 1.;
    const R invN = (R) (1.0 / (double) d.npts);
-   const int c = threadIdx.x % TW, p = threadIdx.x / TW;
+   const int lg = __ffs(TW) - 1;  // TW is a power of two
+   const int c = threadIdx.x & (TW - 1), p = threadIdx.x >> lg;
    int i = 0;
    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, i++) {
       const int q = i % S;
@@ -280,13 +305,22 @@ __global__ void __launch_bounds__(256, 2) k_sweep_xy(const __grid_constant__ CUt
       if (__syncthreads_or(!mbar_wait(&full[q], (i / S) & 1, err))) break;
       P *tile = (P *) (base + q * stage_bytes);
       if (NU) {
+         // every thread keeps one column (blockDim.x is a multiple of TW)
          const int other = t / nzb, z0 = (t - other * nzb) * TW;
          const R *ptile = (const R *) (tile + rows * TW);
-         for (int e = threadIdx.x; e < n * TW; e += blockDim.x) {
-            const int ii = e / TW, cc = e - ii * TW;
-            const int k = z0 + cc;
-            if (k < d.nz) {
-               const R V = (R) (AXIS == 0 ? trap.v(ii, other, k) : trap.v(other, ii, k));
+         const int k = z0 + c;
+         if (k < d.nz) {
+            // Trap::v with the terms of the two fixed coordinates hoisted
+            const double tz = mrn(trap.vl2, trap.z2[k]);
+            const double to = AXIS == 0 ? mrn(trap.vn2, trap.y2[other]) : mrn(trap.vg2, trap.x2[other]);
+            const double *va = AXIS == 0 ? trap.x2 : trap.y2;
+            const double ca = AXIS == 0 ? trap.vg2 : trap.vn2;
+            const int step = blockDim.x >> lg;
+#pragma unroll 2
+            for (int ii = threadIdx.x >> lg; ii < n; ii += step) {
+               const int e = (ii << lg) + c;
+               const double sv = AXIS == 0 ? arn(arn(mrn(ca, va[ii]), to), tz) : arn(arn(to, mrn(ca, va[ii])), tz);
+               const R V = (R) mrn(trap.hp, sv);
                tile[e] = nu_op<R>(scl(tile[e], scale), ptile[e], V, (R) g, (R) gd, (R) dt, invN);
             }
          }
@@ -305,7 +339,7 @@ __global__ void __launch_bounds__(256, 2) k_sweep_xy(const __grid_constant__ CUt
 // its Simpson integral of |psi'|^2 (simpint over z, diffint.cu:106) for the
 // norm of the step.
 template <class R, bool CPLX, bool SIMP, int MSEG, int S>
-__global__ void __launch_bounds__(256, 2) k_sweep_z(typename Tr<R, CPLX>::P *__restrict__ psi, Dims d, SegTab tb,
+__global__ void __launch_bounds__(256, kSweepCtas[0]) k_sweep_z(typename Tr<R, CPLX>::P *__restrict__ psi, Dims d, SegTab tb,
                                                     int TR, int LS, const double *__restrict__ wz, double hz3,
                                                     double *__restrict__ rowsum, uint32_t *err) {
    using P = typename Tr<R, CPLX>::P;
