@@ -25,7 +25,9 @@ struct State {
    double scale;   // pending 1/norm not yet applied to psi (1 when applied)
    double scale2;  // scale * scale, applied to |psi|^2 spectra
    double g, gd;   // couplings of the current step
-   double pad[3];
+   double pad[2];
+   unsigned int ticket;  // CTAs of k_norm_final done (back to 0 after each launch)
+   unsigned int pad_u;
 };
 
 template <class R, bool CPLX> struct Tr {

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <complex>
+#include <type_traits>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -70,6 +71,7 @@ struct gpe_solver {
    int LSr = 0, LSo = 0;                  // shared row strides of the z passes
    CUtensorMap tm_spec_y{}, tm_spec_x{};  // spectrum tiles of the y and x passes
    int boxy = 0, nboxy = 1, boxx = 0, nboxx = 1;
+   int Ly = 8, Lx = 8;  // kz columns per tile of the y and x passes
    size_t esz_psi = 8, esz_c = 16, esz_r = 8;
    void *psi = nullptr, *spec = nullptr, *phi = nullptr;
    void *twx = nullptr, *twy = nullptr, *twz = nullptr;
@@ -324,11 +326,13 @@ static gpe_status make_tmap(CUtensorMap *m, void *base, size_t esz, long w_nz, l
 
 // Lines per CTA and segment length for a sweep over lines of length n with
 // `tw_base` lines filling a 128-byte row: at most 256 threads per CTA.  Lines
-// of 16-byte elements keep 8-point segments (16 would spill registers at
-// three CTAs per SM) and narrow the tile instead.
-static void pick_sweep(int n, int tw_base, bool wide, int &TW, int &MSEG, int &P) {
-   const int ms[2] = {8, 16};
-   const int nms = wide ? 1 : 2;
+// of 16-byte elements keep 8-point segments (16 would spill registers) and
+// narrow the tile instead; 4-byte elements may use 32-point segments, which
+// keep 64-byte tile rows on 512-point lines.
+static void pick_sweep(int n, int tw_base, int esz, int &TW, int &MSEG, int &P) {
+   const bool wide = esz == 16;
+   const int ms[3] = {8, 16, 32};
+   const int nms = wide ? 1 : (esz == 4 ? 3 : 2);
    for (int tw = tw_base; tw >= 2; tw /= 2)
       for (int mi = 0; mi < nms; mi++) {
          const int p = (n - 2 + ms[mi] - 1) / ms[mi];
@@ -347,7 +351,7 @@ static gpe_status setup_sweeps(gpe_solver *s) {
    for (int ax = 0; ax < 3; ax++) {
       auto &w = s->sw[ax];
       int P = 1;
-      pick_sweep((int) nn[ax], tw_base, esz == 16, w.TW, w.MSEG, P);
+      pick_sweep((int) nn[ax], tw_base, (int) esz, w.TW, w.MSEG, P);
       CKS(make_segtab(s, ax, nn[ax], h2[ax], w.MSEG, P));
       const int spw = 32 / w.TW;
       const size_t blk = 2 * (size_t) ((P + spw - 1) / spw + 1) * w.TW * esz;
@@ -377,15 +381,23 @@ static gpe_status setup_sweeps(gpe_solver *s) {
       if (!w.ctas) return fail(GPE_ERR_PARAM, "grid too large for the sweep tiles (shared memory)");
       w.smem = fixed + w.S * stage;
    }
-   // spectrum tiles: spec[x][y][kz] viewed as [nx][ny][2 nzh] scalars
+   // spectrum tiles: spec[x][y][kz] viewed as [nx][ny][2 nzh] scalars; L kz
+   // columns (128-byte rows) per tile, halved down to 4 until the two FFT
+   // buffers of a whole line fit three CTAs on an SM
    {
-      const int L = 128 / (int) s->esz_c;
       s->boxy = (int) std::min<long>(d.ny, 256);
       s->nboxy = (d.ny + s->boxy - 1) / s->boxy;
       s->boxx = (int) std::min<long>(d.nx, 256);
       s->nboxx = (d.nx + s->boxx - 1) / s->boxx;
-      CKS(make_tmap(&s->tm_spec_y, s->spec, rsz, 2 * d.nzh, d.ny, d.nx, 2 * L, s->boxy, 1, 2 * d.nzp));
-      CKS(make_tmap(&s->tm_spec_x, s->spec, rsz, 2 * d.nzh, d.ny, d.nx, 2 * L, 1, s->boxx, 2 * d.nzp));
+      auto pickL = [&](long rows) {
+         int L = 128 / (int) s->esz_c;
+         while (L > 4 && 2 * (size_t) rows * L * s->esz_c > 72 * 1024) L /= 2;
+         return L;
+      };
+      s->Ly = pickL((long) s->boxy * s->nboxy);
+      s->Lx = pickL((long) s->boxx * s->nboxx);
+      CKS(make_tmap(&s->tm_spec_y, s->spec, rsz, 2 * d.nzh, d.ny, d.nx, 2 * s->Ly, s->boxy, 1, 2 * d.nzp));
+      CKS(make_tmap(&s->tm_spec_x, s->spec, rsz, 2 * d.nzh, d.ny, d.nx, 2 * s->Lx, 1, s->boxx, 2 * d.nzp));
    }
    // Simpson weights along z: sum_k wz[k] f[k] * dz / 3 equals simpint (diffint.cu:37-66)
    std::vector<double> wz(d.nz, 0.);
@@ -561,6 +573,37 @@ template <class R, bool CPLX> struct Impl {
       return GPE_OK;
    }
 
+   // runs f(std::integral_constant<int, L>) for the tile width L in {4, 8, 16}
+   template <class F> static gpe_status with_L(int L, F f) {
+      if (L == 16) return f(std::integral_constant<int, 16>());
+      if (L == 8) return f(std::integral_constant<int, 8>());
+      return f(std::integral_constant<int, 4>());
+   }
+
+   template <bool INV, int L> static gpe_status yfft(gpe_solver *s) {
+      const Dims &d = s->d;
+      const int nkb = (d.nzh + L - 1) / L;
+      const size_t smy = 128 + 2 * (size_t) s->boxy * s->nboxy * L * sizeof(C) + d.ny * sizeof(C);
+      CKS(smem_attr((const void *) k_yfft<R, INV, L>, smy));
+      k_yfft<R, INV, L><<<(unsigned) (d.nx * nkb), 256, smy, s->st>>>(s->tm_spec_y, d, s->py, (const C *) s->twy,
+                                                                      s->boxy, s->nboxy, s->err);
+      CKL();
+      mark(s);
+      return GPE_OK;
+   }
+
+   template <int L> static gpe_status xconv(gpe_solver *s) {
+      const Dims &d = s->d;
+      const int nkb = (d.nzh + L - 1) / L;
+      const size_t sm = 128 + 2 * (size_t) s->boxx * s->nboxx * L * sizeof(C) + d.nx * sizeof(C);
+      CKS(smem_attr((const void *) k_xconv<R, L>, sm));
+      k_xconv<R, L><<<(unsigned) (d.ny * nkb), 256, sm, s->st>>>(s->tm_spec_x, d, s->px, (const C *) s->twx, s->udd,
+                                                                 s->state, s->boxx, s->nboxx, s->err);
+      CKL();
+      mark(s);
+      return GPE_OK;
+   }
+
    static gpe_status psidd2(gpe_solver *s) {
       const Dims &d = s->d;
       constexpr int L = FftL<R>::L;
@@ -574,26 +617,9 @@ template <class R, bool CPLX> struct Impl {
          CKL();
          mark(s);
       }
-      const int nkb = (d.nzh + L - 1) / L;
-      const size_t smy = 128 + 2 * (size_t) s->boxy * s->nboxy * L * sizeof(C) + d.ny * sizeof(C);
-      CKS(smem_attr((const void *) k_yfft<R, false>, smy));
-      k_yfft<R, false><<<(unsigned) (d.nx * nkb), 256, smy, s->st>>>(s->tm_spec_y, d, s->py, (const C *) s->twy, s->boxy,
-                                                                     s->nboxy, s->err);
-      CKL();
-      mark(s);
-      {
-         const size_t sm = 128 + 2 * (size_t) s->boxx * s->nboxx * L * sizeof(C) + d.nx * sizeof(C);
-         CKS(smem_attr((const void *) k_xconv<R>, sm));
-         k_xconv<R><<<(unsigned) (d.ny * nkb), 256, sm, s->st>>>(s->tm_spec_x, d, s->px, (const C *) s->twx, s->udd,
-                                                                 s->state, s->boxx, s->nboxx, s->err);
-         CKL();
-         mark(s);
-      }
-      CKS(smem_attr((const void *) k_yfft<R, true>, smy));
-      k_yfft<R, true><<<(unsigned) (d.nx * nkb), 256, smy, s->st>>>(s->tm_spec_y, d, s->py, (const C *) s->twy, s->boxy,
-                                                                    s->nboxy, s->err);
-      CKL();
-      mark(s);
+      CKS(with_L(s->Ly, [&](auto Lc) { return yfft<false, decltype(Lc)::value>(s); }));
+      CKS(with_L(s->Lx, [&](auto Lc) { return xconv<decltype(Lc)::value>(s); }));
+      CKS(with_L(s->Ly, [&](auto Lc) { return yfft<true, decltype(Lc)::value>(s); }));
       {
          const size_t in_el = std::max((size_t) L * d.nzp, ((size_t) L * s->LSo * sizeof(R) + sizeof(C) - 1) / sizeof(C));
          const size_t sm = 128 + ((in_el + 7) & ~(size_t) 7) * sizeof(C) + 2 * (size_t) h * L * sizeof(C) + d.nz * sizeof(C);
@@ -625,8 +651,14 @@ template <class R, bool CPLX> struct Impl {
       return GPE_OK;
    }
 
+   // 32-point segments exist for FP32 real lines only (register budget)
+   static constexpr bool kSeg32 = std::is_same<R, float>::value && !CPLX;
+
    template <int AXIS, bool NU> static gpe_status sweep_xy(gpe_solver *s, double g, double gd) {
       const auto &w = s->sw[AXIS];
+      if constexpr (kSeg32)
+         if (w.MSEG == 32)
+            return w.S == 3 ? sweep_xy_launch<AXIS, NU, 32, 3>(s, g, gd) : sweep_xy_launch<AXIS, NU, 32, 2>(s, g, gd);
       if (w.MSEG == 8) return w.S == 3 ? sweep_xy_launch<AXIS, NU, 8, 3>(s, g, gd) : sweep_xy_launch<AXIS, NU, 8, 2>(s, g, gd);
       return w.S == 3 ? sweep_xy_launch<AXIS, NU, 16, 3>(s, g, gd) : sweep_xy_launch<AXIS, NU, 16, 2>(s, g, gd);
    }
@@ -657,6 +689,11 @@ template <class R, bool CPLX> struct Impl {
    // z sweep; with simp each row also yields its Simpson integral of |psi|^2
    static gpe_status zsweep(gpe_solver *s, bool simp) {
       const auto &w = s->sw[2];
+      if constexpr (kSeg32)
+         if (w.MSEG == 32) {
+            if (w.S == 3) return simp ? sweep_z_launch<true, 32, 3>(s) : sweep_z_launch<false, 32, 3>(s);
+            return simp ? sweep_z_launch<true, 32, 2>(s) : sweep_z_launch<false, 32, 2>(s);
+         }
       if (w.MSEG == 8) {
          if (w.S == 3) return simp ? sweep_z_launch<true, 8, 3>(s) : sweep_z_launch<false, 8, 3>(s);
          return simp ? sweep_z_launch<true, 8, 2>(s) : sweep_z_launch<false, 8, 2>(s);
@@ -666,7 +703,8 @@ template <class R, bool CPLX> struct Impl {
    }
 
    static gpe_status norm_final(gpe_solver *s, double *dev_out) {
-      k_norm_final<<<1, 256, sizeof(double) * s->d.nx, s->st>>>(s->rowA, s->d, s->p.dx, s->p.dy, s->state, dev_out);
+      k_norm_final<<<blocks_for(s->d.nx, kNormRowsPerCta), 32 * kNormRowsPerCta, 0, s->st>>>(
+          s->rowA, s->d, s->p.dx, s->p.dy, s->state, s->tmp, dev_out);
       CKL();
       mark(s);
       s->launches++;

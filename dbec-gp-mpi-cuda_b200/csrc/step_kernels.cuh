@@ -101,12 +101,12 @@ __global__ void __launch_bounds__(256) k_zfwd(const typename Tr<R, CPLX>::P *__r
    }
 }
 
-// Passes 2 and 4: FFT along y of L kz columns of one x plane.
-template <class R, bool INV>
+// Passes 2 and 4: FFT along y of L kz columns of one x plane (L chosen by the
+// host so that three CTAs fit on an SM).
+template <class R, bool INV, int L>
 __global__ void __launch_bounds__(256) k_yfft(const __grid_constant__ CUtensorMap tm, Dims d, FftPlan py,
                                               const cpx<R> *__restrict__ twy, int boxn, int nbox, uint32_t *err) {
    using C = cpx<R>;
-   constexpr int L = FftL<R>::L;
    extern __shared__ __align__(16) unsigned char smem_raw[];
    __shared__ __align__(8) uint64_t bar;
    const int ny = d.ny, rows = boxn * nbox;
@@ -138,13 +138,12 @@ __global__ void __launch_bounds__(256) k_yfft(const __grid_constant__ CUtensorMa
 
 // Pass 3: FFT along x, multiply by Udd(k) * scale^2, inverse FFT along x, for
 // L kz columns of one y plane.  Udd octant layout [|kx|][|ky|][kz].  Compiled
-// for three resident CTAs per SM (their shared tiles fit at nx = 256).
-template <class R>
+// for three resident CTAs per SM (the host picks L so that their tiles fit).
+template <class R, int L>
 __global__ void __launch_bounds__(256, 3) k_xconv(const __grid_constant__ CUtensorMap tm, Dims d, FftPlan px,
                                                const cpx<R> *__restrict__ twx, const double *__restrict__ udd,
                                                const State *__restrict__ st, int boxn, int nbox, uint32_t *err) {
    using C = cpx<R>;
-   constexpr int L = FftL<R>::L;
    extern __shared__ __align__(16) unsigned char smem_raw[];
    __shared__ __align__(8) uint64_t bar;
    const int nx = d.nx, ny = d.ny, rows = boxn * nbox;
@@ -308,19 +307,60 @@ __global__ void k_rows_dens(const typename Tr<R, CPLX>::P *__restrict__ psi, Dim
    if (rowB) rowB[row] = b.finish(hz);
 }
 
+// Weight of sample k in simpint over N samples (src/utils/diffint.cu:37-66),
+// in units of h/3: 1, 4, 2, ..., 4, 1 over the first odd count of samples,
+// plus the end correction (5 f[N-1] + 8 f[N-2] - f[N-3]) / 4 for even N.
+__device__ __forceinline__ double simp_w(int k, int N) {
+   const int mm = (N & 1) ? N : N - 1;
+   double w = k < mm ? ((k == 0 || k == mm - 1) ? 1. : ((k & 1) ? 4. : 2.)) : 0.;
+   if (!(N & 1)) {
+      if (k == N - 1) w += 1.25;
+      else if (k == N - 2) w += 2.;
+      else if (k == N - 3) w -= 0.25;
+   }
+   return w;
+}
+
 // norm = sqrt(S_x S_y rowsum) (calcnorm, imag3d-mpicuda.cu:1194-1218), stores
-// norm, scale = 1/norm and scale^2 in the state.
-__global__ void k_norm_final(const double *__restrict__ rowsum, Dims d, double hx, double hy, State *st,
-                             double *out_norm) {
-   extern __shared__ double tx[];
-   for (int i = threadIdx.x; i < d.nx; i += blockDim.x) tx[i] = simpint_arr(hy, rowsum + (long long) i * d.ny, d.ny);
+// norm, scale = 1/norm and scale^2 in the state.  Each warp forms the
+// weighted Simpson sum over y of one x row (shuffle reduction) into xs[i];
+// the last CTA to finish integrates xs over x.
+constexpr int kNormRowsPerCta = 8;
+__global__ void __launch_bounds__(32 * kNormRowsPerCta) k_norm_final(const double *__restrict__ rowsum, Dims d,
+                                                                     double hx, double hy, State *st, double *xs,
+                                                                     double *out_norm) {
+   const int lane = threadIdx.x & 31;
+   const int i = blockIdx.x * kNormRowsPerCta + (threadIdx.x >> 5);
+   if (i < d.nx) {
+      const double *r = rowsum + (long long) i * d.ny;
+      double a0 = 0., a1 = 0.;
+      int j = lane;
+      for (; j + 32 < d.ny; j += 64) {
+         a0 = fma(simp_w(j, d.ny), r[j], a0);
+         a1 = fma(simp_w(j + 32, d.ny), r[j + 32], a1);
+      }
+      if (j < d.ny) a0 = fma(simp_w(j, d.ny), r[j], a0);
+      double acc = a0 + a1;
+      for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+      if (lane == 0) xs[i] = acc * hy / 3.;
+   }
+   __threadfence();
    __syncthreads();
-   if (threadIdx.x == 0) {
-      const double nrm = sqrt(simpint_arr(hx, tx, d.nx));
+   __shared__ bool last;
+   if (threadIdx.x == 0) last = atomicAdd(&st->ticket, 1u) == gridDim.x - 1;
+   __syncthreads();
+   if (!last || threadIdx.x >= 32) return;
+   __threadfence();
+   double acc = 0.;
+   for (int k = lane; k < d.nx; k += 32) acc = fma(simp_w(k, d.nx), __ldcg(xs + k), acc);
+   for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+   if (lane == 0) {
+      const double nrm = sqrt(acc * hx / 3.);
       const double t = 1. / nrm;
       st->norm = nrm;
       st->scale = t;
       st->scale2 = t * t;
+      st->ticket = 0u;
       if (out_norm) *out_norm = nrm;
    }
 }
