@@ -163,4 +163,70 @@ __device__ C *fft_lines(C *a, C *b, const FftPlan &pl, const C *tw, int twmul) {
    return a;
 }
 
+// In-place variant on one buffer: every thread first reads and transforms
+// all its butterflies of the stage (at most PPT values of the L n points per
+// thread, PPT * blockDim.x >= n L), the CTA synchronises, then every thread
+// writes its results.  Half the shared memory of the ping-pong form, one
+// more barrier per stage.
+template <int RAD, int L, class C, bool INV, int PPT>
+__device__ __forceinline__ void fft_stage_ip(C *buf, int n, int Ns, unsigned magic, const C *__restrict__ tw,
+                                             int twmul) {
+   constexpr int MAXU = (PPT + RAD - 1) / RAD;  // butterflies per thread
+   const int nr = n / RAD;
+   const int nb = nr * L;
+   const int twstep = (n / (Ns * RAD)) * twmul;
+   C v[MAXU][RAD];
+#pragma unroll
+   for (int u = 0; u < MAXU; u++) {
+      const int b = threadIdx.x + u * blockDim.x;
+      if (b < nb) {
+         const int l = b % L;
+         const int j = b / L;
+         const int g = Ns == 1 ? j : (int) __umulhi((unsigned) j, magic);
+         const int k = j - g * Ns;
+         const C *src = buf + j * L + l;
+#pragma unroll
+         for (int t = 0; t < RAD; t++) v[u][t] = src[t * nr * L];
+         if (Ns > 1) {
+#pragma unroll
+            for (int t = 1; t < RAD; t++) {
+               C w = tw[t * k * twstep];
+               if (INV) w.y = -w.y;
+               v[u][t] = cmul(v[u][t], w);
+            }
+         }
+         dftr<RAD, C, INV>(v[u]);
+      }
+   }
+   __syncthreads();
+#pragma unroll
+   for (int u = 0; u < MAXU; u++) {
+      const int b = threadIdx.x + u * blockDim.x;
+      if (b < nb) {
+         const int l = b % L;
+         const int j = b / L;
+         const int g = Ns == 1 ? j : (int) __umulhi((unsigned) j, magic);
+         const int k = j - g * Ns;
+         C *dst = buf + (g * Ns * RAD + k) * L + l;
+#pragma unroll
+         for (int t = 0; t < RAD; t++) dst[t * Ns * L] = v[u][t];
+      }
+   }
+   __syncthreads();
+}
+
+// Full in-place transform of L interleaved lines in buf (PPT as above).
+template <int L, class C, bool INV, int PPT>
+__device__ void fft_lines_ip(C *buf, const FftPlan &pl, const C *tw, int twmul) {
+   // make_plan orders the stages by radix (8, 4, 2, 3, 5): one loop per radix
+   // (a switch over the radix inside one loop made ptxas spill the values
+   // held across the barriers)
+   int st = 0;
+   for (; st < pl.nst && pl.rad[st] == 8; st++) fft_stage_ip<8, L, C, INV, PPT>(buf, pl.n, pl.ns[st], pl.magic[st], tw, twmul);
+   for (; st < pl.nst && pl.rad[st] == 4; st++) fft_stage_ip<4, L, C, INV, PPT>(buf, pl.n, pl.ns[st], pl.magic[st], tw, twmul);
+   for (; st < pl.nst && pl.rad[st] == 2; st++) fft_stage_ip<2, L, C, INV, PPT>(buf, pl.n, pl.ns[st], pl.magic[st], tw, twmul);
+   for (; st < pl.nst && pl.rad[st] == 3; st++) fft_stage_ip<3, L, C, INV, PPT>(buf, pl.n, pl.ns[st], pl.magic[st], tw, twmul);
+   for (; st < pl.nst && pl.rad[st] == 5; st++) fft_stage_ip<5, L, C, INV, PPT>(buf, pl.n, pl.ns[st], pl.magic[st], tw, twmul);
+}
+
 }  // namespace gpe

@@ -382,16 +382,18 @@ static gpe_status setup_sweeps(gpe_solver *s) {
       w.smem = fixed + w.S * stage;
    }
    // spectrum tiles: spec[x][y][kz] viewed as [nx][ny][2 nzh] scalars; L kz
-   // columns (128-byte rows) per tile, halved down to 4 until the two FFT
-   // buffers of a whole line fit three CTAs on an SM
+   // columns (128-byte rows) per tile, halved (down to 2) until a tile of a
+   // whole line holds at most 256 PPT points (32 KB), the in-place FFT's
+   // register budget
    {
       s->boxy = (int) std::min<long>(d.ny, 256);
       s->nboxy = (d.ny + s->boxy - 1) / s->boxy;
       s->boxx = (int) std::min<long>(d.nx, 256);
       s->nboxx = (d.nx + s->boxx - 1) / s->boxx;
+      const long ppt = s->fp32 ? 16 : 8;  // FftL<R>::PPT
       auto pickL = [&](long rows) {
          int L = 128 / (int) s->esz_c;
-         while (L > 4 && 2 * (size_t) rows * L * s->esz_c > 72 * 1024) L /= 2;
+         while (L > 2 && rows * L > 256 * ppt) L /= 2;
          return L;
       };
       s->Ly = pickL((long) s->boxy * s->nboxy);
@@ -573,17 +575,26 @@ template <class R, bool CPLX> struct Impl {
       return GPE_OK;
    }
 
-   // runs f(std::integral_constant<int, L>) for the tile width L in {4, 8, 16}
+   // runs f(std::integral_constant<int, v>) for v in {2, 4, 8, 16} (tile
+   // widths) or {8, 16, 32} (points per thread)
    template <class F> static gpe_status with_L(int L, F f) {
       if (L == 16) return f(std::integral_constant<int, 16>());
       if (L == 8) return f(std::integral_constant<int, 8>());
-      return f(std::integral_constant<int, 4>());
+      if (L == 4) return f(std::integral_constant<int, 4>());
+      return f(std::integral_constant<int, 2>());
    }
+   template <class F> static gpe_status with_ppt(int ppt, F f) {
+      if (ppt <= 8) return f(std::integral_constant<int, 8>());
+      if (ppt <= 16) return f(std::integral_constant<int, 16>());
+      return f(std::integral_constant<int, 32>());
+   }
+   // points per thread of the z passes: (nz/2) L over 256 threads
+   static int zppt(const gpe_solver *s) { return (int) (((s->d.nz / 2) * FftL<R>::L + 255) / 256); }
 
    template <bool INV, int L> static gpe_status yfft(gpe_solver *s) {
       const Dims &d = s->d;
       const int nkb = (d.nzh + L - 1) / L;
-      const size_t smy = 128 + 2 * (size_t) s->boxy * s->nboxy * L * sizeof(C) + d.ny * sizeof(C);
+      const size_t smy = 128 + (size_t) s->boxy * s->nboxy * L * sizeof(C) + d.ny * sizeof(C);
       CKS(smem_attr((const void *) k_yfft<R, INV, L>, smy));
       k_yfft<R, INV, L><<<(unsigned) (d.nx * nkb), 256, smy, s->st>>>(s->tm_spec_y, d, s->py, (const C *) s->twy,
                                                                       s->boxy, s->nboxy, s->err);
@@ -595,7 +606,7 @@ template <class R, bool CPLX> struct Impl {
    template <int L> static gpe_status xconv(gpe_solver *s) {
       const Dims &d = s->d;
       const int nkb = (d.nzh + L - 1) / L;
-      const size_t sm = 128 + 2 * (size_t) s->boxx * s->nboxx * L * sizeof(C) + d.nx * sizeof(C);
+      const size_t sm = 128 + (size_t) s->boxx * s->nboxx * L * sizeof(C) + d.nx * sizeof(C);
       CKS(smem_attr((const void *) k_xconv<R, L>, sm));
       k_xconv<R, L><<<(unsigned) (d.ny * nkb), 256, sm, s->st>>>(s->tm_spec_x, d, s->px, (const C *) s->twx, s->udd,
                                                                  s->state, s->boxx, s->nboxx, s->err);
@@ -610,24 +621,29 @@ template <class R, bool CPLX> struct Impl {
       const int h = d.nz / 2;
       C *spec = (C *) s->spec;
       const unsigned grows = blocks_for(d.nxy, L);
-      {
-         const size_t sm = 128 + (size_t) L * s->LSr * sizeof(P) + 2 * (size_t) h * L * sizeof(C) + d.nz * sizeof(C);
-         CKS(smem_attr((const void *) k_zfwd<R, CPLX>, sm));
-         k_zfwd<R, CPLX><<<grows, 256, sm, s->st>>>((const P *) s->psi, spec, d, s->ph, (const C *) s->twz, s->LSr, s->err);
+      CKS(with_ppt(zppt(s), [&](auto pc) {
+         constexpr int PPT = decltype(pc)::value;
+         const size_t sm = 128 + (size_t) L * s->LSr * sizeof(P) + (size_t) h * L * sizeof(C) + d.nz * sizeof(C);
+         CKS(smem_attr((const void *) k_zfwd<R, CPLX, PPT>, sm));
+         k_zfwd<R, CPLX, PPT><<<grows, 256, sm, s->st>>>((const P *) s->psi, spec, d, s->ph, (const C *) s->twz, s->LSr,
+                                                         s->err);
          CKL();
          mark(s);
-      }
+         return GPE_OK;
+      }));
       CKS(with_L(s->Ly, [&](auto Lc) { return yfft<false, decltype(Lc)::value>(s); }));
       CKS(with_L(s->Lx, [&](auto Lc) { return xconv<decltype(Lc)::value>(s); }));
       CKS(with_L(s->Ly, [&](auto Lc) { return yfft<true, decltype(Lc)::value>(s); }));
-      {
+      CKS(with_ppt(zppt(s), [&](auto pc) {
+         constexpr int PPT = decltype(pc)::value;
          const size_t in_el = std::max((size_t) L * d.nzp, ((size_t) L * s->LSo * sizeof(R) + sizeof(C) - 1) / sizeof(C));
-         const size_t sm = 128 + ((in_el + 7) & ~(size_t) 7) * sizeof(C) + 2 * (size_t) h * L * sizeof(C) + d.nz * sizeof(C);
-         CKS(smem_attr((const void *) k_zinv<R>, sm));
-         k_zinv<R><<<grows, 256, sm, s->st>>>(spec, (R *) s->phi, d, s->ph, (const C *) s->twz, s->LSo, s->err);
+         const size_t sm = 128 + ((in_el + 7) & ~(size_t) 7) * sizeof(C) + (size_t) h * L * sizeof(C) + d.nz * sizeof(C);
+         CKS(smem_attr((const void *) k_zinv<R, PPT>, sm));
+         k_zinv<R, PPT><<<grows, 256, sm, s->st>>>(spec, (R *) s->phi, d, s->ph, (const C *) s->twz, s->LSo, s->err);
          CKL();
          mark(s);
-      }
+         return GPE_OK;
+      }));
       k_phifix<R><<<256, 256, 0, s->st>>>((R *) s->phi, d);
       CKL();
       mark(s);

@@ -21,7 +21,13 @@ namespace gpe {
 // interleaved layout the FFT engine works in.
 // ===========================================================================
 
-template <class R> struct FftL { static constexpr int L = 128 / (2 * (int) sizeof(R)); };
+// L: lines per tile of the z passes (128-byte rows); PPT: points per thread
+// of the y and x passes, whose tile width the host picks so that a tile of a
+// whole line holds at most 256 PPT points (32 KB).
+template <class R> struct FftL {
+   static constexpr int L = 128 / (2 * (int) sizeof(R));
+   static constexpr int PPT = sizeof(R) == 8 ? 8 : 16;
+};
 
 // |psi|^2 of L rows (row stride LS elements) packed as complex lines of
 // length h = nz/2 in the interleaved layout: buf[m L + l] = (rho[2m], rho[2m+1]).
@@ -57,8 +63,8 @@ __device__ __forceinline__ void zfwd_split(const cpx<R> *Z, const cpx<R> *tw, in
 }
 
 // Pass 1: |psi|^2 rows -> half spectrum rows (L rows per CTA).
-template <class R, bool CPLX>
-__global__ void __launch_bounds__(256) k_zfwd(const typename Tr<R, CPLX>::P *__restrict__ psi,
+template <class R, bool CPLX, int PPT>
+__global__ void __launch_bounds__(256, 4) k_zfwd(const typename Tr<R, CPLX>::P *__restrict__ psi,
                                               cpx<R> *__restrict__ spec, Dims d, FftPlan ph,
                                               const cpx<R> *__restrict__ twz, int LSr, uint32_t *err) {
    using C = cpx<R>;
@@ -67,11 +73,10 @@ __global__ void __launch_bounds__(256) k_zfwd(const typename Tr<R, CPLX>::P *__r
    extern __shared__ __align__(16) unsigned char smem_raw[];
    __shared__ __align__(8) uint64_t bar;
    const int nz = d.nz, h = nz / 2, nzh = d.nzh, nzp = d.nzp;
-   // layout: rows [L][LSr] (later the output rows [L][nzp]) | bufA | bufB | twiddles
+   // layout: rows [L][LSr] (later the output rows [L][nzp]) | FFT buffer | twiddles
    P *rows = (P *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
-   C *bufA = (C *) (rows + L * LSr);
-   C *bufB = bufA + h * L;
-   C *tw = bufB + h * L;
+   C *buf = (C *) (rows + L * LSr);
+   C *tw = buf + h * L;
    const long long r0 = (long long) blockIdx.x * L;
    const int nr = (int) ((d.nxy - r0) < L ? (d.nxy - r0) : L);
    const uint32_t row_bytes = (uint32_t) (nz * sizeof(P));
@@ -87,11 +92,11 @@ __global__ void __launch_bounds__(256) k_zfwd(const typename Tr<R, CPLX>::P *__r
    }
    for (int e = threadIdx.x; e < (L - nr) * LSr; e += blockDim.x) rows[nr * LSr + e] = zero_of<P>();
    if (__syncthreads_or(!mbar_wait(&bar, 0, err))) return;
-   zfwd_pack<R, CPLX, L>(rows, LSr, bufA, h);
+   zfwd_pack<R, CPLX, L>(rows, LSr, buf, h);
    __syncthreads();
-   const C *Z = fft_lines<L, C, false>(bufA, bufB, ph, tw, 2);
+   fft_lines_ip<L, C, false, PPT>(buf, ph, tw, 2);
    C *out = (C *) rows;  // [L][nzp]; the rows are no longer read
-   zfwd_split<R, L>(Z, tw, h, nzh, nzp, out, nzp, L);
+   zfwd_split<R, L>(buf, tw, h, nzh, nzp, out, nzp, L);
    fence_proxy_async();
    __syncthreads();
    if (threadIdx.x == 0) {
@@ -104,15 +109,15 @@ __global__ void __launch_bounds__(256) k_zfwd(const typename Tr<R, CPLX>::P *__r
 // Passes 2 and 4: FFT along y of L kz columns of one x plane (L chosen by the
 // host so that three CTAs fit on an SM).
 template <class R, bool INV, int L>
-__global__ void __launch_bounds__(256) k_yfft(const __grid_constant__ CUtensorMap tm, Dims d, FftPlan py,
-                                              const cpx<R> *__restrict__ twy, int boxn, int nbox, uint32_t *err) {
+__global__ void __launch_bounds__(256, 4) k_yfft(const __grid_constant__ CUtensorMap tm, Dims d, FftPlan py,
+                                                 const cpx<R> *__restrict__ twy, int boxn, int nbox, uint32_t *err) {
    using C = cpx<R>;
+   constexpr int PPT = FftL<R>::PPT;
    extern __shared__ __align__(16) unsigned char smem_raw[];
    __shared__ __align__(8) uint64_t bar;
    const int ny = d.ny, rows = boxn * nbox;
-   C *bufA = (C *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
-   C *bufB = bufA + rows * L;
-   C *tw = bufB + rows * L;
+   C *buf = (C *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
+   C *tw = buf + rows * L;
    const int nkb = (d.nzh + L - 1) / L;
    const int x = blockIdx.x / nkb, k0 = (blockIdx.x - x * nkb) * L;
    if (threadIdx.x == 0) {
@@ -123,14 +128,14 @@ __global__ void __launch_bounds__(256) k_yfft(const __grid_constant__ CUtensorMa
    if (threadIdx.x == 0) {
       mbar_arrive_expect_tx(&bar, (uint32_t) (rows * L * sizeof(C) + ny * sizeof(C)));
       bulk_load(tw, twy, (uint32_t) (ny * sizeof(C)), &bar);
-      for (int b = 0; b < nbox; b++) tma_load_3d(bufA + b * boxn * L, &tm, 2 * k0, b * boxn, x, &bar);
+      for (int b = 0; b < nbox; b++) tma_load_3d(buf + b * boxn * L, &tm, 2 * k0, b * boxn, x, &bar);
    }
    if (__syncthreads_or(!mbar_wait(&bar, 0, err))) return;
-   C *res = fft_lines<L, C, INV>(bufA, bufB, py, tw, 1);
+   fft_lines_ip<L, C, INV, PPT>(buf, py, tw, 1);
    fence_proxy_async();
    __syncthreads();
    if (threadIdx.x == 0) {
-      for (int b = 0; b < nbox; b++) tma_store_3d(&tm, 2 * k0, b * boxn, x, res + b * boxn * L);
+      for (int b = 0; b < nbox; b++) tma_store_3d(&tm, 2 * k0, b * boxn, x, buf + b * boxn * L);
       bulk_commit();
       bulk_wait_all();
    }
@@ -140,16 +145,16 @@ __global__ void __launch_bounds__(256) k_yfft(const __grid_constant__ CUtensorMa
 // L kz columns of one y plane.  Udd octant layout [|kx|][|ky|][kz].  Compiled
 // for three resident CTAs per SM (the host picks L so that their tiles fit).
 template <class R, int L>
-__global__ void __launch_bounds__(256, 3) k_xconv(const __grid_constant__ CUtensorMap tm, Dims d, FftPlan px,
-                                               const cpx<R> *__restrict__ twx, const double *__restrict__ udd,
-                                               const State *__restrict__ st, int boxn, int nbox, uint32_t *err) {
+__global__ void __launch_bounds__(256, 4) k_xconv(const __grid_constant__ CUtensorMap tm, Dims d, FftPlan px,
+                                                  const cpx<R> *__restrict__ twx, const double *__restrict__ udd,
+                                                  const State *__restrict__ st, int boxn, int nbox, uint32_t *err) {
    using C = cpx<R>;
+   constexpr int PPT = FftL<R>::PPT;
    extern __shared__ __align__(16) unsigned char smem_raw[];
    __shared__ __align__(8) uint64_t bar;
    const int nx = d.nx, ny = d.ny, rows = boxn * nbox;
-   C *bufA = (C *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
-   C *bufB = bufA + rows * L;
-   C *tw = bufB + rows * L;
+   C *buf = (C *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
+   C *tw = buf + rows * L;
    const int nkb = (d.nzh + L - 1) / L;
    const int y = blockIdx.x / nkb, k0 = (blockIdx.x - y * nkb) * L;
    if (threadIdx.x == 0) {
@@ -160,11 +165,11 @@ __global__ void __launch_bounds__(256, 3) k_xconv(const __grid_constant__ CUtens
    if (threadIdx.x == 0) {
       mbar_arrive_expect_tx(&bar, (uint32_t) (rows * L * sizeof(C) + nx * sizeof(C)));
       bulk_load(tw, twx, (uint32_t) (nx * sizeof(C)), &bar);
-      for (int b = 0; b < nbox; b++) tma_load_3d(bufA + b * boxn * L, &tm, 2 * k0, y, b * boxn, &bar);
+      for (int b = 0; b < nbox; b++) tma_load_3d(buf + b * boxn * L, &tm, 2 * k0, y, b * boxn, &bar);
    }
    if (__syncthreads_or(!mbar_wait(&bar, 0, err))) return;
-   C *res = fft_lines<L, C, false>(bufA, bufB, px, tw, 1);
-   C *oth = (res == bufA) ? bufB : bufA;
+   fft_lines_ip<L, C, false, PPT>(buf, px, tw, 1);
+   C *res = buf;
    const double s2 = st->scale2;
    const int nyh = ny / 2 + 1, nzh = d.nzh;
    const int ay = (y <= ny / 2) ? y : ny - y;
@@ -176,31 +181,30 @@ __global__ void __launch_bounds__(256, 3) k_xconv(const __grid_constant__ CUtens
       res[e] = cscale(res[e], u);
    }
    __syncthreads();
-   C *fin = fft_lines<L, C, true>(res, oth, px, tw, 1);
+   fft_lines_ip<L, C, true, PPT>(buf, px, tw, 1);
    fence_proxy_async();
    __syncthreads();
    if (threadIdx.x == 0) {
-      for (int b = 0; b < nbox; b++) tma_store_3d(&tm, 2 * k0, y, b * boxn, fin + b * boxn * L);
+      for (int b = 0; b < nbox; b++) tma_store_3d(&tm, 2 * k0, y, b * boxn, buf + b * boxn * L);
       bulk_commit();
       bulk_wait_all();
    }
 }
 
 // Pass 5: half spectrum rows -> phi rows (unnormalised inverse, Hermitian).
-template <class R>
-__global__ void __launch_bounds__(256) k_zinv(const cpx<R> *__restrict__ spec, R *__restrict__ phi, Dims d,
-                                              FftPlan ph, const cpx<R> *__restrict__ twz, int LSo, uint32_t *err) {
+template <class R, int PPT>
+__global__ void __launch_bounds__(256, 4) k_zinv(const cpx<R> *__restrict__ spec, R *__restrict__ phi, Dims d,
+                                                 FftPlan ph, const cpx<R> *__restrict__ twz, int LSo, uint32_t *err) {
    using C = cpx<R>;
    constexpr int L = FftL<R>::L;
    extern __shared__ __align__(16) unsigned char smem_raw[];
    __shared__ __align__(8) uint64_t bar;
    const int nz = d.nz, h = nz / 2, nzp = d.nzp;
-   // layout: input rows [L][nzp] (later the phi rows [L][LSo]) | bufA | bufB | twiddles
+   // layout: input rows [L][nzp] (later the phi rows [L][LSo]) | FFT buffer | twiddles
    C *in = (C *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
    const int in_elems = ((L * nzp) > (L * LSo + 1) / 2 ? (L * nzp) : (L * LSo + 1) / 2);
-   C *bufA = in + ((in_elems + 7) & ~7);
-   C *bufB = bufA + h * L;
-   C *tw = bufB + h * L;
+   C *buf = in + ((in_elems + 7) & ~7);
+   C *tw = buf + h * L;
    const long long r0 = (long long) blockIdx.x * L;
    const int nr = (int) ((d.nxy - r0) < L ? (d.nxy - r0) : L);
    if (threadIdx.x == 0) {
@@ -223,10 +227,11 @@ __global__ void __launch_bounds__(256) k_zinv(const cpx<R> *__restrict__ spec, R
       b = cconj(b);
       const C E = cadd(a, b);
       const C O = cmul(csub(a, b), cconj(tw[k]));
-      bufA[e] = mk<R>(E.x - O.y, E.y + O.x);
+      buf[e] = mk<R>(E.x - O.y, E.y + O.x);
    }
    __syncthreads();
-   const C *z = fft_lines<L, C, true>(bufA, bufB, ph, tw, 2);
+   fft_lines_ip<L, C, true, PPT>(buf, ph, tw, 2);
+   const C *z = buf;
    R *out = (R *) in;  // [L][LSo]
    for (int e = threadIdx.x; e < h * L; e += blockDim.x) {
       const int l = e % L, m = e / L;
