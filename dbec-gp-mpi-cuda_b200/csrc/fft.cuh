@@ -10,11 +10,11 @@
 // 128-byte row: bank-conflict free.  This is also the layout a TMA box of L
 // columns by the whole line lands in.
 //
-// Each radix-r stage (autosort Stockham, decimation in time) reads one
-// buffer and writes the other:
+// Each radix-r stage (autosort Stockham, decimation in time) computes
 //   j in [0, n/r), k = j mod Ns,  v[t] = src[j + t n/r] * W^(t k n/(Ns r))
 //   v = DFT_r(v),  dst[(j / Ns) Ns r + k + t Ns] = v[t],  Ns *= r
-// leaving the result in natural order.  W = exp(-2 pi i / n) comes from a
+// leaving the result in natural order; src and dst are the same buffer, the
+// reads of a stage finishing (barrier) before its writes start.  W = exp(-2 pi i / n) comes from a
 // table of the n-th roots computed on the host in long double (twmul > 1
 // reads a table of a longer transform with stride twmul).  Inverse
 // transforms use conjugated twiddles and are unnormalised, like cuFFT's
@@ -111,63 +111,11 @@ template <int R, class C, bool INV> __device__ __forceinline__ void dftr(C *v) {
    else dft8<C, INV>(v);
 }
 
-// One Stockham stage over L interleaved lines.
-template <int RAD, int L, class C, bool INV>
-__device__ __forceinline__ void fft_stage(const C *__restrict__ src, C *__restrict__ dst, int n, int Ns,
-                                          unsigned magic, const C *__restrict__ tw, int twmul) {
-   const int nr = n / RAD;
-   const int nb = nr * L;
-   const int twstep = (n / (Ns * RAD)) * twmul;
-   for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-      const int l = b % L;  // L is a power of two
-      const int j = b / L;
-      const int g = Ns == 1 ? j : (int) __umulhi((unsigned) j, magic);  // j / Ns
-      const int k = j - g * Ns;
-      C v[RAD];
-      const C *s = src + j * L + l;
-#pragma unroll
-      for (int t = 0; t < RAD; t++) v[t] = s[t * nr * L];
-      if (Ns > 1) {
-#pragma unroll
-         for (int t = 1; t < RAD; t++) {
-            C w = tw[t * k * twstep];
-            if (INV) w.y = -w.y;
-            v[t] = cmul(v[t], w);
-         }
-      }
-      dftr<RAD, C, INV>(v);
-      C *d = dst + (g * Ns * RAD + k) * L + l;
-#pragma unroll
-      for (int t = 0; t < RAD; t++) d[t * Ns * L] = v[t];
-   }
-}
-
-// Full transform of L interleaved lines; returns the buffer (a or b) holding
-// the result.  All threads of the CTA call it; it synchronises after every
-// stage.
-template <int L, class C, bool INV>
-__device__ C *fft_lines(C *a, C *b, const FftPlan &pl, const C *tw, int twmul) {
-   for (int st = 0; st < pl.nst; st++) {
-      const int Ns = pl.ns[st];
-      const unsigned mg = pl.magic[st];
-      switch (pl.rad[st]) {
-      case 2: fft_stage<2, L, C, INV>(a, b, pl.n, Ns, mg, tw, twmul); break;
-      case 3: fft_stage<3, L, C, INV>(a, b, pl.n, Ns, mg, tw, twmul); break;
-      case 4: fft_stage<4, L, C, INV>(a, b, pl.n, Ns, mg, tw, twmul); break;
-      case 5: fft_stage<5, L, C, INV>(a, b, pl.n, Ns, mg, tw, twmul); break;
-      default: fft_stage<8, L, C, INV>(a, b, pl.n, Ns, mg, tw, twmul); break;
-      }
-      __syncthreads();
-      C *t = a; a = b; b = t;
-   }
-   return a;
-}
-
-// In-place variant on one buffer: every thread first reads and transforms
-// all its butterflies of the stage (at most PPT values of the L n points per
+// One stage on one buffer: every thread first reads and transforms all its
+// butterflies of the stage (at most PPT values of the L n points per
 // thread, PPT * blockDim.x >= n L), the CTA synchronises, then every thread
-// writes its results.  Half the shared memory of the ping-pong form, one
-// more barrier per stage.
+// writes its results.  Half the shared memory of a ping-pong pair of
+// buffers, for one more barrier per stage.
 template <int RAD, int L, class C, bool INV, int PPT>
 __device__ __forceinline__ void fft_stage_ip(C *buf, int n, int Ns, unsigned magic, const C *__restrict__ tw,
                                              int twmul) {
