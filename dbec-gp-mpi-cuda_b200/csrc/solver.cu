@@ -324,21 +324,23 @@ static gpe_status make_tmap(CUtensorMap *m, void *base, size_t esz, long w_nz, l
    return GPE_OK;
 }
 
-// Lines per CTA and segment length for a sweep over lines of length n with
-// `tw_base` lines filling a 128-byte row: at most 256 threads per CTA.  Lines
-// of 16-byte elements keep 8-point segments (16 would spill registers) and
-// narrow the tile instead; 4-byte elements may use 32-point segments, which
-// keep 64-byte tile rows on 512-point lines.
-static void pick_sweep(int n, int tw_base, int esz, int &TW, int &MSEG, int &P) {
+// Candidate (lines per CTA TW, segment length MSEG, segments P) for a sweep
+// over lines of length n, widest tile first: TW from `tw_base` (a 128-byte
+// row) down to 2, at most 256 threads (TW * P).  Lines of 16-byte elements
+// keep 8-point segments (16 would spill registers); 4-byte elements may use
+// 32-point segments, which keep 64-byte tile rows on 512-point lines.
+static int sweep_candidates(int n, int tw_base, int esz, int *TW, int *MSEG, int *P, int cap) {
    const bool wide = esz == 16;
    const int ms[3] = {8, 16, 32};
    const int nms = wide ? 1 : (esz == 4 ? 3 : 2);
-   for (int tw = tw_base; tw >= 2; tw /= 2)
-      for (int mi = 0; mi < nms; mi++) {
+   int k = 0;
+   for (int tw = tw_base; tw >= 2 && k < cap; tw /= 2)
+      for (int mi = 0; mi < nms && k < cap; mi++) {
          const int p = (n - 2 + ms[mi] - 1) / ms[mi];
-         if (tw * p <= 256) { TW = tw; MSEG = ms[mi]; P = p; return; }
+         if (tw * p <= 256) { TW[k] = tw; MSEG[k] = ms[mi]; P[k] = p; k++; break; }
       }
-   TW = 2; MSEG = wide ? 8 : 16; P = (n - 2 + MSEG - 1) / MSEG;
+   if (k == 0) { TW[0] = 2; MSEG[0] = wide ? 8 : 16; P[0] = (n - 2 + MSEG[0] - 1) / MSEG[0]; k = 1; }
+   return k;
 }
 
 static gpe_status setup_sweeps(gpe_solver *s) {
@@ -348,32 +350,49 @@ static gpe_status setup_sweeps(gpe_solver *s) {
    const int tw_base = (int) (128 / esz);
    const long nn[3] = {d.nx, d.ny, d.nz};
    const double h2[3] = {s->p.dx * s->p.dx, s->p.dy * s->p.dy, s->p.dz * s->p.dz};
+   const size_t sm_cap = 227 * 1024;
    for (int ax = 0; ax < 3; ax++) {
       auto &w = s->sw[ax];
-      int P = 1;
-      pick_sweep((int) nn[ax], tw_base, (int) esz, w.TW, w.MSEG, P);
+      // the widest tile for which as many CTAs as the kernels are compiled for
+      // fit on an SM with a 2-stage pipeline (else the widest tile, fewer CTAs)
+      const int max_ctas = kSweepCtas[ax == 0 ? 1 : 0];
+      int cTW[8], cM[8], cP[8];
+      const int nc = sweep_candidates((int) nn[ax], tw_base, (int) esz, cTW, cM, cP, 8);
+      auto sizes = [&](int TW, int P, size_t &stage, size_t &fixed) {
+         const int spw = 32 / TW;
+         const size_t blk = 2 * (size_t) ((P + spw - 1) / spw + 1) * TW * esz;
+         if (ax < 2) {
+            const long rows = (long) std::min<long>(nn[ax], 256) * ((nn[ax] + 255) / 256);
+            stage = (rows * TW * esz + (ax == 0 ? rows * TW * rsz : 0) + 127) & ~(size_t) 127;
+            fixed = 128 + blk;
+         } else {
+            stage = ((size_t) TW * (d.nz + 16 / esz) * esz + 127) & ~(size_t) 127;
+            fixed = 128 + blk + (size_t) P * TW * sizeof(double);
+         }
+      };
+      int pick = 0;
+      for (int c = 0; c < nc; c++) {
+         size_t st_, fx_;
+         sizes(cTW[c], cP[c], st_, fx_);
+         if ((fx_ + 2 * st_) * max_ctas <= sm_cap) { pick = c; break; }
+      }
+      w.TW = cTW[pick];
+      w.MSEG = cM[pick];
+      const int P = cP[pick];
       CKS(make_segtab(s, ax, nn[ax], h2[ax], w.MSEG, P));
-      const int spw = 32 / w.TW;
-      const size_t blk = 2 * (size_t) ((P + spw - 1) / spw + 1) * w.TW * esz;
       size_t stage = 0, fixed = 0;
+      sizes(w.TW, P, stage, fixed);
       if (ax < 2) {
          w.boxn = (int) std::min<long>(nn[ax], 256);
          w.nbox = (int) ((nn[ax] + w.boxn - 1) / w.boxn);
-         const long rows = (long) w.boxn * w.nbox;
          const int by = ax == 1 ? w.boxn : 1, bx = ax == 0 ? w.boxn : 1;
          CKS(make_tmap(&w.tm_psi, s->psi, s->fp32 ? 4 : 8, E * d.nz, d.ny, d.nx, E * w.TW, by, bx));
          CKS(make_tmap(&w.tm_phi, s->phi, rsz, d.nz, d.ny, d.nx, w.TW, by, bx));
-         stage = (rows * w.TW * esz + (ax == 0 ? rows * w.TW * rsz : 0) + 127) & ~(size_t) 127;
-         fixed = 128 + blk;
       } else {
          w.LS = (int) (d.nz + 16 / esz);
-         stage = ((size_t) w.TW * w.LS * esz + 127) & ~(size_t) 127;
-         fixed = 128 + blk + (size_t) P * w.TW * sizeof(double);
       }
-      // as many resident CTAs as the kernels are compiled for and shared
-      // memory allows, then the deepest pipeline (2 or 3 stages) that keeps them
-      const size_t sm_cap = 227 * 1024;
-      const int max_ctas = kSweepCtas[ax == 0 ? 1 : 0];
+      // as many resident CTAs as allowed, then the deepest pipeline (2 or 3
+      // stages) that keeps them
       w.ctas = 0;
       for (int ct = max_ctas; ct >= 1 && !w.ctas; ct--)
          for (int S = 3; S >= 2 && !w.ctas; S--)
