@@ -27,8 +27,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
                   "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC]
 
-LIB_SOURCES = ["solver.cu", "noalloc.cu"]
-LIB_DEPS = ["solver.cu", "noalloc.cu", "common.cuh", "fft.cuh", "kernels.cuh", "step_kernels.cuh", "sweep_kernels.cuh", "tma.cuh"]
+LIB_SOURCES = ["solver.cu", "noalloc.cu", "batch.cu", "server.cpp"]
+LIB_DEPS = LIB_SOURCES + ["common.cuh", "fft.cuh", "kernels.cuh", "step_kernels.cuh", "sweep_kernels.cuh", "tma.cuh",
+                          "internal.h"]
 HOST_COMMON = ["cfg.cpp", "cli.cpp"]
 PROGRAMS = {"imag3d-mpicuda": "imag3d_main.cpp", "real3d-mpicuda": "real3d_main.cpp"}
 
@@ -53,7 +54,7 @@ def build_lib(force=False, verbose_ptxas=False):
     if force or _stale(LIB, deps):
         extra = ["-Xptxas", "-v"] if verbose_ptxas else []
         _run([NVCC] + NVFLAGS + extra + ["-shared", "-o", LIB] +
-             [os.path.join(CSRC, f) for f in LIB_SOURCES] + ["-lcudart"])
+             [os.path.join(CSRC, f) for f in LIB_SOURCES] + ["-lcudart", "-lpthread"])
     return LIB
 
 

@@ -1,0 +1,28 @@
+// internal.h -- hooks of the solver handle for the batch runner and the
+// request server, which live in the same library (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "gpe.h"
+
+namespace gpe {
+
+void set_last_error(const std::string &msg);
+// Queues nsteps split steps at fixed couplings on the handle's stream, with no
+// synchronisation; in imaginary time the last renormalisation stays pending.
+gpe_status queue_steps(gpe_solver *s, long nsteps, double g, double gd);
+// Queues the pending renormalisation (imaginary time; nothing in real time).
+gpe_status queue_finish(gpe_solver *s);
+// Queues calcmuen into the handle's observable slots; read_muen synchronises
+// the stream and returns mu and E.
+gpe_status queue_muen(gpe_solver *s, double g, double gd);
+gpe_status read_muen(gpe_solver *s, double *mu, double *en);
+cudaStream_t stream_of(gpe_solver *s);
+gpe_status params_of(gpe_solver *s, gpe_params *p);
+int device_of(gpe_solver *s);
+long long kernels_per_step(gpe_solver *s);
+
+}  // namespace gpe

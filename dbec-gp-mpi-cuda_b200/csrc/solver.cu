@@ -16,6 +16,7 @@
 #include <cudaTypedefs.h>
 
 #include "gpe.h"
+#include "internal.h"
 #include "step_kernels.cuh"
 #include "sweep_kernels.cuh"
 
@@ -72,6 +73,7 @@ struct gpe_solver {
    CUtensorMap tm_spec_y{}, tm_spec_x{};  // spectrum tiles of the y and x passes
    int boxy = 0, nboxy = 1, boxx = 0, nboxx = 1;
    int Ly = 8, Lx = 8;  // kz columns per tile of the y and x passes
+   gpe_tuning tune{};   // requested tile configuration (0 = default heuristic)
    size_t esz_psi = 8, esz_c = 16, esz_r = 8;
    void *psi = nullptr, *spec = nullptr, *phi = nullptr;
    void *twx = nullptr, *twy = nullptr, *twz = nullptr;
@@ -107,13 +109,17 @@ static void mark(gpe_solver *s) {
 }
 
 // ---------------------------------------------------------------- planning
-static bool make_plan(int n, FftPlan &pl) {
+// Radices in the order the stages are grouped (fft_lines_ip loops over them
+// in this order); max_radix 4 or 2 drops the larger powers of two.
+static bool make_plan(int n, FftPlan &pl, int max_radix = 8) {
    pl.n = n;
    pl.nst = 0;
    int m = n;
    static const int pref[] = {8, 4, 2, 3, 5};
-   for (int r : pref)
+   for (int r : pref) {
+      if ((r == 8 || r == 4) && r > max_radix) continue;
       while (m % r == 0 && pl.nst < kMaxStages) { pl.rad[pl.nst++] = r; m /= r; }
+   }
    int ns = 1;
    for (int st = 0; st < pl.nst; st++) {
       pl.ns[st] = ns;
@@ -343,7 +349,10 @@ static int sweep_candidates(int n, int tw_base, int esz, int *TW, int *MSEG, int
    return k;
 }
 
-static gpe_status setup_sweeps(gpe_solver *s) {
+// Tile configuration of the sweeps and of the y / x FFT passes, and the FFT
+// plans: the heuristics below, or the values of s->tune where set.  May be
+// called again (gpe_set_tuning); it reuploads only the segment tables.
+static gpe_status plan_tiles(gpe_solver *s) {
    const Dims &d = s->d;
    const size_t esz = s->esz_psi, rsz = s->esz_r;
    const int E = s->cplx ? 2 : 1;
@@ -371,14 +380,24 @@ static gpe_status setup_sweeps(gpe_solver *s) {
          }
       };
       int pick = 0;
-      for (int c = 0; c < nc; c++) {
-         size_t st_, fx_;
-         sizes(cTW[c], cP[c], st_, fx_);
-         if ((fx_ + 2 * st_) * max_ctas <= sm_cap) { pick = c; break; }
+      if (s->tune.sweep_tw[ax] > 0) {
+         pick = -1;
+         for (int c = 0; c < nc; c++)
+            if (cTW[c] == s->tune.sweep_tw[ax]) pick = c;
+         if (pick < 0) return fail(GPE_ERR_PARAM, "tuning: sweep_tw not available for this line length");
+      } else {
+         for (int c = 0; c < nc; c++) {
+            size_t st_, fx_;
+            sizes(cTW[c], cP[c], st_, fx_);
+            if ((fx_ + 2 * st_) * max_ctas <= sm_cap) { pick = c; break; }
+         }
       }
       w.TW = cTW[pick];
       w.MSEG = cM[pick];
       const int P = cP[pick];
+      if (w.M) cudaFree(w.M);
+      if (w.N) cudaFree(w.N);
+      w.M = w.N = nullptr;
       CKS(make_segtab(s, ax, nn[ax], h2[ax], w.MSEG, P));
       size_t stage = 0, fixed = 0;
       sizes(w.TW, P, stage, fixed);
@@ -393,9 +412,12 @@ static gpe_status setup_sweeps(gpe_solver *s) {
       }
       // as many resident CTAs as allowed, then the deepest pipeline (2 or 3
       // stages) that keeps them
+      const int s_hi = s->tune.sweep_stages[ax] > 0 ? s->tune.sweep_stages[ax] : 3;
+      const int s_lo = s->tune.sweep_stages[ax] > 0 ? s->tune.sweep_stages[ax] : 2;
+      if (s_lo < 2 || s_hi > 3) return fail(GPE_ERR_PARAM, "tuning: sweep_stages must be 2 or 3");
       w.ctas = 0;
       for (int ct = max_ctas; ct >= 1 && !w.ctas; ct--)
-         for (int S = 3; S >= 2 && !w.ctas; S--)
+         for (int S = s_hi; S >= s_lo && !w.ctas; S--)
             if ((fixed + S * stage) * ct <= sm_cap) { w.ctas = ct; w.S = S; }
       if (!w.ctas) return fail(GPE_ERR_PARAM, "grid too large for the sweep tiles (shared memory)");
       w.smem = fixed + w.S * stage;
@@ -417,9 +439,30 @@ static gpe_status setup_sweeps(gpe_solver *s) {
       };
       s->Ly = pickL((long) s->boxy * s->nboxy);
       s->Lx = pickL((long) s->boxx * s->nboxx);
+      const long rows[2] = {(long) s->boxy * s->nboxy, (long) s->boxx * s->nboxx};
+      int *Ls[2] = {&s->Ly, &s->Lx};
+      for (int a = 0; a < 2; a++) {
+         const int L = s->tune.fft_tile[a];
+         if (L == 0) continue;
+         if ((L & (L - 1)) || L < 2 || L > 128 / (int) s->esz_c || rows[a] * L > 256 * ppt)
+            return fail(GPE_ERR_PARAM, "tuning: fft_tile must be a power of two, >= 2, at most a 128-byte row and "
+                                       "at most 256 PPT points per tile");
+         *Ls[a] = L;
+      }
+      const int mr = s->tune.fft_max_radix > 0 ? s->tune.fft_max_radix : 8;
+      if (mr != 8 && mr != 4 && mr != 2) return fail(GPE_ERR_PARAM, "tuning: fft_max_radix must be 8, 4 or 2");
+      make_plan(d.nx, s->px, mr);
+      make_plan(d.ny, s->py, mr);
+      make_plan(d.nz / 2, s->ph, mr);
       CKS(make_tmap(&s->tm_spec_y, s->spec, rsz, 2 * d.nzh, d.ny, d.nx, 2 * s->Ly, s->boxy, 1, 2 * d.nzp));
       CKS(make_tmap(&s->tm_spec_x, s->spec, rsz, 2 * d.nzh, d.ny, d.nx, 2 * s->Lx, 1, s->boxx, 2 * d.nzp));
    }
+   return GPE_OK;
+}
+
+// Simpson weights along z and the device status word (once per handle).
+static gpe_status setup_static(gpe_solver *s) {
+   const Dims &d = s->d;
    // Simpson weights along z: sum_k wz[k] f[k] * dz / 3 equals simpint (diffint.cu:37-66)
    std::vector<double> wz(d.nz, 0.);
    const int N = d.nz, mm = (N % 2) ? N : N - 1;
@@ -497,9 +540,6 @@ static gpe_status create_impl(const gpe_params *p, void *stream, gpe_solver *s) 
    d.nzp = s->fp32 ? (d.nzh + 1) & ~1 : d.nzh;
    d.nxy = (long long) d.nx * d.ny;
    d.npts = d.nxy * d.nz;
-   make_plan(d.nx, s->px);
-   make_plan(d.ny, s->py);
-   make_plan(d.nz / 2, s->ph);
    const size_t r = s->fp32 ? 4 : 8;
    s->esz_r = r;
    s->esz_c = 2 * r;
@@ -529,7 +569,8 @@ static gpe_status create_impl(const gpe_params *p, void *stream, gpe_solver *s) 
    CKS(make_coef(s, 1, d.ny, p->dy * p->dy));
    CKS(make_coef(s, 2, d.nz, p->dz * p->dz));
    CKS(make_udd(s));
-   CKS(setup_sweeps(s));
+   CKS(plan_tiles(s));
+   CKS(setup_static(s));
 
    // space mesh (initpsi, imag3d-mpicuda.cu:842-855)
    const long nx2 = d.nx / 2, ny2 = d.ny / 2, nz2 = d.nz / 2;
@@ -1278,3 +1319,166 @@ extern "C" gpe_status gpe_profile_step(gpe_solver *s, long nsteps, double g, dou
    for (auto &x : ev) cudaEventDestroy(x);
    return st;
 }
+
+// ------------------------------------------------------------------ tuning
+extern "C" gpe_status gpe_get_tuning(gpe_solver *s, gpe_tuning *t) {
+   CHECK_HANDLE(s);
+   if (!t) return fail(GPE_ERR_PARAM, "null tuning");
+   for (int a = 0; a < 3; a++) {
+      t->sweep_tw[a] = s->sw[a].TW;
+      t->sweep_stages[a] = s->sw[a].S;
+   }
+   t->fft_tile[0] = s->Ly;
+   t->fft_tile[1] = s->Lx;
+   t->fft_max_radix = s->tune.fft_max_radix > 0 ? s->tune.fft_max_radix : 8;
+   return GPE_OK;
+}
+
+extern "C" gpe_status gpe_set_tuning(gpe_solver *s, const gpe_tuning *t) {
+   CHECK_HANDLE(s);
+   CK(cudaSetDevice(s->dev));
+   CK(cudaStreamSynchronize(s->st));  // queued kernels still read the old tables
+   const gpe_tuning old = s->tune;
+   s->tune = t ? *t : gpe_tuning{};
+   gpe_status st = plan_tiles(s);
+   if (st != GPE_OK) {
+      const std::string msg = g_err;
+      s->tune = old;
+      plan_tiles(s);
+      return fail(st, msg);
+   }
+   return GPE_OK;
+}
+
+// Per-kernel times of the step (index as gpe_step_kernel_name) for the
+// configuration in use; psi advances by warm + nsteps steps.
+static gpe_status time_kernels(gpe_solver *s, double g, double gd, int nsteps, double *ms) {
+   double warm[10];
+   int cnt = 0;
+   CKS(gpe_profile_step(s, 1, g, gd, warm, 10, &cnt));
+   return gpe_profile_step(s, nsteps, g, gd, ms, 10, &cnt);
+}
+
+extern "C" gpe_status gpe_autotune(gpe_solver *s, double g, double gd, int nsteps, gpe_tuning *best) {
+   CHECK_HANDLE(s);
+   if (nsteps < 1) return fail(GPE_ERR_PARAM, "autotune needs nsteps >= 1");
+   CK(cudaSetDevice(s->dev));
+   // keep psi and the step state
+   const size_t pbytes = s->esz_psi * (size_t) s->d.npts;
+   void *save = nullptr;
+   CK(cudaMalloc(&save, pbytes));
+   State st_save;
+   cudaError_t e = cudaMemcpyAsync(save, s->psi, pbytes, cudaMemcpyDeviceToDevice, s->st);
+   if (e == cudaSuccess) e = cudaMemcpyAsync(&st_save, s->state, sizeof(State), cudaMemcpyDeviceToHost, s->st);
+   if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+   if (e != cudaSuccess) {
+      cudaFree(save);
+      return fail(GPE_ERR_CUDA, cudaGetErrorString(e));
+   }
+   const gpe_tuning start = s->tune;
+   gpe_tuning pick = start;
+   double best_sweep[3] = {1e30, 1e30, 1e30}, best_y = 1e30, best_x = 1e30, best_fft = 1e30;
+   const int ksw[3] = {6, 7, 8};  // x, y, z sweeps in the kernel list
+   gpe_status st = GPE_OK;
+   // sweeps: every available lines-per-CTA value with both pipeline depths
+   {
+      const long nn[3] = {s->d.nx, s->d.ny, s->d.nz};
+      int cTW[3][8], cM[8], cP[8], nc[3];
+      for (int a = 0; a < 3; a++)
+         nc[a] = sweep_candidates((int) nn[a], (int) (128 / s->esz_psi), (int) s->esz_psi, cTW[a], cM, cP, 8);
+      const int ncmax = std::max(nc[0], std::max(nc[1], nc[2]));
+      for (int c = 0; c < ncmax && st == GPE_OK; c++)
+         for (int S = 2; S <= 3 && st == GPE_OK; S++) {
+            gpe_tuning t = start;
+            for (int a = 0; a < 3; a++) {
+               t.sweep_tw[a] = cTW[a][std::min(c, nc[a] - 1)];
+               t.sweep_stages[a] = S;
+            }
+            s->tune = t;
+            if (plan_tiles(s) != GPE_OK) continue;  // does not fit: skip
+            double ms[10];
+            st = time_kernels(s, g, gd, nsteps, ms);
+            for (int a = 0; a < 3 && st == GPE_OK; a++)
+               if (ms[ksw[a]] < best_sweep[a]) {
+                  best_sweep[a] = ms[ksw[a]];
+                  pick.sweep_tw[a] = t.sweep_tw[a];
+                  pick.sweep_stages[a] = S;
+               }
+         }
+   }
+   // FFT: tile widths of the y and x passes, then the largest radix
+   for (int L = 128 / (int) s->esz_c; L >= 2 && st == GPE_OK; L /= 2) {
+      gpe_tuning t = pick;
+      t.fft_tile[0] = t.fft_tile[1] = L;
+      s->tune = t;
+      if (plan_tiles(s) != GPE_OK) continue;
+      double ms[10];
+      st = time_kernels(s, g, gd, nsteps, ms);
+      if (st != GPE_OK) break;
+      if (ms[1] + ms[3] < best_y) { best_y = ms[1] + ms[3]; pick.fft_tile[0] = L; }
+      if (ms[2] < best_x) { best_x = ms[2]; pick.fft_tile[1] = L; }
+   }
+   for (int r = 8; r >= 2 && st == GPE_OK; r /= 2) {
+      gpe_tuning t = pick;
+      t.fft_max_radix = r;
+      s->tune = t;
+      if (plan_tiles(s) != GPE_OK) continue;
+      double ms[10];
+      st = time_kernels(s, g, gd, nsteps, ms);
+      if (st != GPE_OK) break;
+      const double f = ms[0] + ms[1] + ms[2] + ms[3] + ms[4];
+      if (f < best_fft) { best_fft = f; pick.fft_max_radix = r; }
+   }
+   s->tune = st == GPE_OK ? pick : start;
+   gpe_status st2 = plan_tiles(s);
+   e = cudaMemcpyAsync(s->psi, save, pbytes, cudaMemcpyDeviceToDevice, s->st);
+   if (e == cudaSuccess) e = cudaMemcpyAsync(s->state, &st_save, sizeof(State), cudaMemcpyHostToDevice, s->st);
+   if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+   cudaFree(save);
+   if (st != GPE_OK) return st;
+   if (st2 != GPE_OK) return st2;
+   if (e != cudaSuccess) return fail(GPE_ERR_CUDA, cudaGetErrorString(e));
+   if (best) *best = s->tune;
+   return GPE_OK;
+}
+
+// ------------------------------------------------------ hooks (internal.h)
+namespace gpe {
+
+gpe_status queue_steps(gpe_solver *s, long nsteps, double g, double gd) {
+   CHECK_HANDLE(s);
+   for (long c = 0; c < nsteps; c++) CKS(DISPATCH(s, step(s, g, gd, nullptr)));
+   return GPE_OK;
+}
+
+gpe_status queue_finish(gpe_solver *s) {
+   CHECK_HANDLE(s);
+   if (!s->cplx) return DISPATCH(s, apply_scale(s));
+   return GPE_OK;
+}
+
+gpe_status queue_muen(gpe_solver *s, double g, double gd) {
+   CHECK_HANDLE(s);
+   return DISPATCH(s, muen(s, g, gd, s->obs + 8));
+}
+
+gpe_status read_muen(gpe_solver *s, double *mu, double *en) {
+   CHECK_HANDLE(s);
+   double v[2];
+   CKS(read_obs(s, v, 2, 8));
+   CKS(check_err(s));
+   if (mu) *mu = v[0];
+   if (en) *en = v[1];
+   return GPE_OK;
+}
+
+cudaStream_t stream_of(gpe_solver *s) { return s->st; }
+gpe_status params_of(gpe_solver *s, gpe_params *p) {
+   CHECK_HANDLE(s);
+   *p = s->p;
+   return GPE_OK;
+}
+int device_of(gpe_solver *s) { return s->dev; }
+long long kernels_per_step(gpe_solver *s) { return s->cplx ? 9 : 10; }
+
+}  // namespace gpe

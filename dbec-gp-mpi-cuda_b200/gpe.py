@@ -36,6 +36,30 @@ class Params(C.Structure):
                 ("gamma", C.c_double), ("nu", C.c_double), ("lamda", C.c_double), ("cutoff", C.c_double)]
 
 
+class Tuning(C.Structure):
+    """gpe_tuning: tile configuration (0 = built-in heuristic)."""
+    _fields_ = [("sweep_tw", C.c_int * 3), ("sweep_stages", C.c_int * 3), ("fft_tile", C.c_int * 2),
+                ("fft_max_radix", C.c_int)]
+
+    def as_dict(self):
+        return {"sweep_tw": list(self.sweep_tw), "sweep_stages": list(self.sweep_stages),
+                "fft_tile": list(self.fft_tile), "fft_max_radix": self.fft_max_radix}
+
+
+REQ_GROUND, REQ_EVOLVE = 0, 1
+
+
+class Request(C.Structure):
+    _fields_ = [("p", Params), ("kind", C.c_int), ("g", C.c_double), ("gd", C.c_double), ("tol", C.c_double),
+                ("check_every", C.c_long), ("max_steps", C.c_long)]
+
+
+class Result(C.Structure):
+    _fields_ = [("id", C.c_longlong), ("status", C.c_int), ("steps", C.c_long), ("mu", C.c_double),
+                ("en", C.c_double), ("norm", C.c_double), ("rms", C.c_double * 4), ("t_submit", C.c_double),
+                ("t_start", C.c_double), ("t_done", C.c_double)]
+
+
 # every symbol include/gpe.h declares, with (restype, argtypes)
 _P = C.c_void_p
 _D = C.c_double
@@ -68,6 +92,22 @@ _SIGS = {
     "gpe_step_kernel_name": (C.c_char_p, [_P, C.c_int]),
     "gpe_step_kernel_bytes": (C.c_double, [_P, C.c_int]),
     "gpe_norm_noalloc": (C.c_int, [_P, C.c_int, C.c_long, C.c_long, C.c_long, _D, _D, _D, _P, _P]),
+    "gpe_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
+    "gpe_set_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
+    "gpe_autotune": (C.c_int, [_P, _D, _D, C.c_int, C.POINTER(Tuning)]),
+    "gpe_batch_create": (C.c_int, [C.POINTER(Params), _DP, _DP, C.c_int, C.POINTER(_P)]),
+    "gpe_batch_destroy": (None, [_P]),
+    "gpe_batch_solver": (C.c_int, [_P, C.c_int, C.POINTER(_P)]),
+    "gpe_batch_set_couplings": (C.c_int, [_P, _DP, _DP]),
+    "gpe_batch_autotune": (C.c_int, [_P, C.c_int]),
+    "gpe_batch_run": (C.c_int, [_P, C.c_long]),
+    "gpe_batch_time_steps": (C.c_int, [_P, C.c_long, _DP]),
+    "gpe_batch_launch_count": (C.c_int, [_P, C.POINTER(C.c_longlong)]),
+    "gpe_server_create": (C.c_int, [C.c_int, C.c_longlong, C.c_int, C.POINTER(_P)]),
+    "gpe_server_destroy": (None, [_P]),
+    "gpe_server_submit": (C.c_int, [_P, C.POINTER(Request), C.POINTER(C.c_longlong)]),
+    "gpe_server_wait": (C.c_int, [_P, C.c_longlong, _D, C.POINTER(Result)]),
+    "gpe_server_stats": (C.c_int, [_P, _DP]),
 }
 
 _lib = None
@@ -255,3 +295,118 @@ class Solver:
         ms = C.c_double()
         _check(lib().gpe_time_steps(self.h, int(nsteps), float(g), float(gd), C.byref(ms)))
         return ms.value
+
+    # -- tile configuration --------------------------------------------------
+    def get_tuning(self) -> Tuning:
+        t = Tuning()
+        _check(lib().gpe_get_tuning(self.h, C.byref(t)))
+        return t
+
+    def set_tuning(self, t: Tuning | None):
+        _check(lib().gpe_set_tuning(self.h, C.byref(t) if t is not None else None))
+
+    def autotune(self, g, gd, nsteps=3) -> Tuning:
+        t = Tuning()
+        _check(lib().gpe_autotune(self.h, float(g), float(gd), int(nsteps), C.byref(t)))
+        return t
+
+
+class _Borrowed(Solver):
+    """Handle owned by a batch: never destroyed from Python."""
+
+    def __init__(self, h, params):
+        self.params = params
+        self.shape = (params.nx, params.ny, params.nz)
+        self.mode = params.mode
+        self.h = h
+
+    def close(self):
+        self.h = None
+
+
+class Batch:
+    """gpe_batch: independent solves stepped together (one CUDA graph per step)."""
+
+    def __init__(self, params, g, gd):
+        n = len(params)
+        arr = (Params * n)(*params)
+        ga = (C.c_double * n)(*[float(x) for x in g])
+        gda = (C.c_double * n)(*[float(x) for x in gd])
+        h = C.c_void_p()
+        _check(lib().gpe_batch_create(arr, ga, gda, n, C.byref(h)))
+        self.h = h
+        self.params = list(params)
+        self.n = n
+
+    def solver(self, i) -> Solver:
+        hs = C.c_void_p()
+        _check(lib().gpe_batch_solver(self.h, int(i), C.byref(hs)))
+        return _Borrowed(hs, self.params[i])
+
+    def set_couplings(self, g, gd):
+        ga = (C.c_double * self.n)(*[float(x) for x in g])
+        gda = (C.c_double * self.n)(*[float(x) for x in gd])
+        _check(lib().gpe_batch_set_couplings(self.h, ga, gda))
+
+    def autotune(self, nsteps=3):
+        _check(lib().gpe_batch_autotune(self.h, int(nsteps)))
+
+    def run(self, nsteps):
+        _check(lib().gpe_batch_run(self.h, int(nsteps)))
+
+    def time_steps(self, nsteps):
+        ms = C.c_double()
+        _check(lib().gpe_batch_time_steps(self.h, int(nsteps), C.byref(ms)))
+        return ms.value
+
+    def launch_count(self):
+        v = C.c_longlong()
+        _check(lib().gpe_batch_launch_count(self.h, C.byref(v)))
+        return v.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().gpe_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """gpe_server: request server with continuous batching."""
+
+    def __init__(self, budget_bytes, max_active=64, device=-1):
+        h = C.c_void_p()
+        _check(lib().gpe_server_create(int(device), int(budget_bytes), int(max_active), C.byref(h)))
+        self.h = h
+
+    def submit(self, params: Params, kind, g, gd, tol=1e-8, check_every=100, max_steps=100000) -> int:
+        rq = Request(params, int(kind), float(g), float(gd), float(tol), int(check_every), int(max_steps))
+        i = C.c_longlong()
+        _check(lib().gpe_server_submit(self.h, C.byref(rq), C.byref(i)))
+        return i.value
+
+    def wait(self, rid, timeout=-1.0) -> Result:
+        r = Result()
+        _check(lib().gpe_server_wait(self.h, int(rid), float(timeout), C.byref(r)))
+        return r
+
+    def stats(self):
+        v = (C.c_double * 4)()
+        _check(lib().gpe_server_stats(self.h, v))
+        return {"done": v[0], "peak_active": v[1], "peak_bytes": v[2], "chunks": v[3]}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().gpe_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -134,6 +134,92 @@ gpe_status gpe_profile_step(gpe_solver *s, long nsteps, double g, double gd, dou
 const char *gpe_step_kernel_name(gpe_solver *s, int i);
 double gpe_step_kernel_bytes(gpe_solver *s, int i);
 
+/* Tile configuration of a handle (no reference counterpart: the reference
+ * has one fixed cuFFT + one-thread-per-line layout).  Zero fields select the
+ * built-in heuristic. */
+typedef struct gpe_tuning {
+   int sweep_tw[3];     /* lines per CTA of the x, y, z sweeps (a power of two) */
+   int sweep_stages[3]; /* TMA pipeline depth of the x, y, z sweeps: 2 or 3 */
+   int fft_tile[2];     /* kz columns per tile of the y and x FFT passes */
+   int fft_max_radix;   /* largest radix of the FFT plans: 8, 4 or 2 */
+} gpe_tuning;
+/* The configuration in use (every field filled in). */
+gpe_status gpe_get_tuning(gpe_solver *s, gpe_tuning *t);
+/* Re-plans the tiles with t (NULL = all defaults); psi and the state are kept.
+ * GPE_ERR_PARAM (and the previous configuration restored) when a value does not
+ * fit this grid. */
+gpe_status gpe_set_tuning(gpe_solver *s, const gpe_tuning *t);
+/* Autotuner: times candidate configurations with gpe_profile_step (nsteps
+ * steps each at couplings g, gd) and keeps, per sweep axis, the fastest lines
+ * per CTA and pipeline depth, and for the FFT passes the fastest tile widths
+ * and largest radix.  psi and the state are restored afterwards; the chosen
+ * configuration is applied and returned in *best (may be NULL). */
+gpe_status gpe_autotune(gpe_solver *s, double g, double gd, int nsteps, gpe_tuning *best);
+
+/* ---------------------------------------------------------------- batch
+ * Many independent solves with their own grids and parameters (no reference
+ * counterpart: the reference runs one solve per MPI job).  Each instance is a
+ * full handle (its own stream and device memory); one batch step runs one
+ * split step of every instance: the instances' kernels, captured once into a
+ * CUDA graph with one branch per instance, are relaunched as one graph per
+ * step, so small instances run concurrently on the GPU. */
+typedef struct gpe_batch gpe_batch;
+/* params[i] and couplings g[i], gd[i] of instance i (n >= 1). */
+gpe_status gpe_batch_create(const gpe_params *params, const double *g, const double *gd, int n, gpe_batch **out);
+void gpe_batch_destroy(gpe_batch *b);
+/* The handle of instance i (owned by the batch): initial state, observables. */
+gpe_status gpe_batch_solver(gpe_batch *b, int i, gpe_solver **s);
+/* New couplings for every instance (the step graph is captured again). */
+gpe_status gpe_batch_set_couplings(gpe_batch *b, const double *g, const double *gd);
+/* Autotunes one instance per distinct (grid, mode, precision) with
+ * gpe_autotune (nsteps per trial) and applies its choice to the others. */
+gpe_status gpe_batch_autotune(gpe_batch *b, int nsteps);
+/* nsteps batch steps, then the pending renormalisation of imaginary-time
+ * instances; returns after the GPU finished. */
+gpe_status gpe_batch_run(gpe_batch *b, long nsteps);
+/* nsteps batch steps bracketed by CUDA events: elapsed milliseconds. */
+gpe_status gpe_batch_time_steps(gpe_batch *b, long nsteps, double *ms);
+/* Kernel launches executed by batch steps so far. */
+gpe_status gpe_batch_launch_count(gpe_batch *b, long long *count);
+
+/* --------------------------------------------------------------- server
+ * Request server with continuous batching (no reference counterpart).  A
+ * worker thread admits queued requests while the summed gpe_device_bytes of
+ * the active solves stays within the HBM budget and fewer than max_active are
+ * running, keeps each psi resident on the device, runs all active solves
+ * concurrently in chunks (each on its own stream), and retires a solve when it
+ * has converged (ground state) or done its steps (evolution); requests that
+ * arrive meanwhile are admitted at the next chunk boundary. */
+typedef struct gpe_server gpe_server;
+enum { GPE_REQ_GROUND = 0, GPE_REQ_EVOLVE = 1 };
+typedef struct gpe_request {
+   gpe_params p;       /* p.mode: GPE_MODE_IMAG for GROUND, GPE_MODE_REAL for EVOLVE */
+   int kind;           /* GPE_REQ_GROUND or GPE_REQ_EVOLVE */
+   double g, gd;       /* couplings */
+   double tol;         /* GROUND: stop when |mu_k - mu_{k-1}| / |mu_k| < tol between checks */
+   long check_every;   /* GROUND: steps between mu checks; EVOLVE: steps per chunk */
+   long max_steps;     /* GROUND: step cap; EVOLVE: steps to run */
+} gpe_request;
+typedef struct gpe_result {
+   long long id;
+   int status;         /* gpe_status of the solve */
+   long steps;         /* steps run */
+   double mu, en;      /* calcmuen at the end */
+   double norm;        /* calcnorm at the end (before any renormalisation) */
+   double rms[4];      /* calcrms at the end */
+   double t_submit, t_start, t_done;  /* seconds since the server started */
+} gpe_result;
+/* device: CUDA ordinal (-1 = current); hbm_budget_bytes: admission budget. */
+gpe_status gpe_server_create(int device, long long hbm_budget_bytes, int max_active, gpe_server **out);
+/* Stops the worker after the queued and active requests finished. */
+void gpe_server_destroy(gpe_server *sv);
+gpe_status gpe_server_submit(gpe_server *sv, const gpe_request *rq, long long *id);
+/* Waits (at most timeout_s seconds, < 0 = forever) for request id; fills res.
+ * GPE_ERR_TIMEOUT when it has not finished in time. */
+gpe_status gpe_server_wait(gpe_server *sv, long long id, double timeout_s, gpe_result *res);
+/* stats[0] requests done, [1] peak active, [2] peak bytes admitted, [3] chunks run. */
+gpe_status gpe_server_stats(gpe_server *sv, double *stats);
+
 /* Norm of a device-resident psi with no device allocation.  No counterpart in
  * the reference: it serves callers that cannot call cudaMalloc where they need
  * the norm (a latency-critical loop that must not take cudaMalloc/cudaFree's

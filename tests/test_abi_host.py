@@ -138,3 +138,22 @@ def test_cli_density_needs_outstp_and_potmem_range(programs, tmp_path):
     f.write_text(BASE + "DYNAOUT = dyn\n")
     r = _cli("real3d-mpicuda", ["-i", str(f)], tmp_path)
     assert r.returncode == 1 and r.stderr.strip() == "OUTSTPT is not defined in the configuration file."
+
+
+def test_server_rejects_bad_requests_on_the_host(gpe_lib):
+    """Request validation happens at submission, before any GPU work."""
+    gpe = gpe_lib
+    with pytest.raises(gpe.GpeError) as e:
+        gpe.Server(0)
+    assert e.value.status == 1
+    sv = gpe.Server(1 << 30, device=0)
+    imag = gpe.make_params(0, 16, 16, 16, .2, .2, .2, .004, 1., 1., 1., 1.6)
+    real = gpe.make_params(1, 16, 16, 16, .2, .2, .2, .004, 1., 1., 1., 1.6)
+    bad_grid = gpe.make_params(0, 14, 16, 16, .2, .2, .2, .004, 1., 1., 1., 1.6)
+    cases = [(real, gpe.REQ_GROUND, {}), (imag, gpe.REQ_EVOLVE, {}), (bad_grid, gpe.REQ_GROUND, {}),
+             (imag, gpe.REQ_GROUND, {"check_every": 0}), (imag, 7, {})]
+    for p, kind, kw in cases:
+        with pytest.raises(gpe.GpeError) as e:
+            sv.submit(p, kind, 1., 0., **kw)
+        assert e.value.status == 1
+    sv.close()

@@ -1,0 +1,177 @@
+"""Tile tuning, the batch runner and the request server (GPU).
+
+* tuning: another tile configuration gives the same step to rounding
+  (<= 1e-12 relative), a bad one is refused and the old one kept; the
+  autotuner leaves psi untouched;
+* batch: a batch step is exactly each instance's own step (bitwise equal to
+  running the instances one by one through gpe_run);
+* server: a ground-state request gives the same result (bitwise) whether it
+  runs alone or among other requests, the HBM budget bounds the concurrent
+  solves, and a request larger than the budget is refused with
+  GPE_ERR_BUDGET; the server's ground state equals gpe_run in the same chunks.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+OP_TOL = 1e-12
+
+
+def rel(a, b):
+    return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / max(np.max(np.abs(np.asarray(b))), 1e-300))
+
+
+def params(gpe, mode, shape, dx=0.25, trap=(0.5, 1.0, 1.5), dt=None, prec=0):
+    nx, ny, nz = shape
+    dt = 0.1 * dx * dx if dt is None else dt
+    return gpe.make_params(mode, nx, ny, nz, dx, dx, dx, dt, *trap, 0.5 * min(shape) * dx, precision=prec)
+
+
+def test_tuning_changes_only_rounding(gpe_lib):
+    gpe = gpe_lib
+    p = params(gpe, 1, (48, 40, 32), dt=4e-4)
+    a, b = gpe.Solver(p), gpe.Solver(p)
+    t = b.get_tuning()
+    assert all(v > 0 for v in t.sweep_tw) and t.fft_max_radix == 8
+    t2 = gpe.Tuning()
+    t2.sweep_tw[0] = max(2, t.sweep_tw[0] // 2)
+    t2.sweep_stages[1] = 2
+    t2.fft_tile[0] = 2
+    t2.fft_max_radix = 4
+    b.set_tuning(t2)
+    got = b.get_tuning()
+    assert got.sweep_tw[0] == t2.sweep_tw[0] and got.fft_tile[0] == 2 and got.fft_max_radix == 4
+    for s in (a, b):
+        s.init_gaussian()
+        s.run(20, 60., 20.)
+    assert rel(b.get_psi(), a.get_psi()) <= OP_TOL
+    bad = gpe.Tuning()
+    bad.sweep_tw[2] = 3
+    with pytest.raises(gpe.GpeError) as e:
+        b.set_tuning(bad)
+    assert e.value.status == 1
+    assert b.get_tuning().fft_tile[0] == 2  # previous configuration kept
+    a.close()
+    b.close()
+
+
+def test_autotune_keeps_psi(gpe_lib):
+    gpe = gpe_lib
+    s = gpe.Solver(params(gpe, 0, (64, 64, 64)))
+    s.init_gaussian()
+    s.calcnorm(True)
+    s.run(5, 100., 30.)
+    before = s.get_psi()
+    best = s.autotune(100., 30., nsteps=2)
+    assert all(v > 0 for v in best.sweep_tw)
+    assert np.array_equal(s.get_psi(), before)
+    s.run(5, 100., 30.)
+    s.close()
+
+
+def _instances(gpe):
+    ps = [params(gpe, 0, (32, 32, 32)), params(gpe, 1, (48, 40, 32), dx=0.2, dt=4e-4, trap=(1., 1., 4.)),
+          params(gpe, 0, (24, 20, 30), dx=0.3, trap=(1., 0.7, 2.)), params(gpe, 1, (32, 32, 32), dt=5e-4)]
+    g = [100., 60., 40., 80.]
+    gd = [30., 20., 10., 50.]
+    return ps, g, gd
+
+
+def test_batch_equals_individual_runs(gpe_lib):
+    gpe = gpe_lib
+    ps, g, gd = _instances(gpe)
+    b = gpe.Batch(ps, g, gd)
+    for i in range(len(ps)):
+        s = b.solver(i)
+        s.init_gaussian()
+        if ps[i].mode == 0:
+            s.calcnorm(True)
+    b.run(12)
+    b.run(3)
+    assert b.launch_count() == 15 * sum(10 if p.mode == 0 else 9 for p in ps)
+    for i, p in enumerate(ps):
+        s = gpe.Solver(p)
+        s.init_gaussian()
+        if p.mode == 0:
+            s.calcnorm(True)
+        s.run(12, g[i], gd[i])
+        s.run(3, g[i], gd[i])
+        assert np.array_equal(s.get_psi(), b.solver(i).get_psi()), i
+        s.close()
+    b.close()
+
+
+def _ground(gpe, shape, g, gd):
+    return dict(params=params(gpe, 0, shape), kind=gpe.REQ_GROUND, g=g, gd=gd, tol=1e-6, check_every=50,
+                max_steps=3000)
+
+
+def _submit(sv, rq):
+    return sv.submit(rq["params"], rq["kind"], rq["g"], rq["gd"], rq["tol"], rq["check_every"], rq["max_steps"])
+
+
+def _fields(r):
+    return (r.status, r.steps, r.mu, r.en, r.norm, tuple(r.rms))
+
+
+def test_server_result_same_alone_and_in_mix(gpe_lib):
+    gpe = gpe_lib
+    target = _ground(gpe, (32, 32, 32), 80., 20.)
+    sv = gpe.Server(8 << 30)
+    alone = sv.wait(_submit(sv, target), timeout=120)
+    sv.close()
+    assert alone.status == 0 and alone.steps > 50
+    sv = gpe.Server(8 << 30)
+    others = [dict(params=params(gpe, 1, (40, 40, 32), dt=5e-4), kind=gpe.REQ_EVOLVE, g=60., gd=20., tol=0.,
+                   check_every=100, max_steps=400),
+              _ground(gpe, (48, 48, 32), 120., 30.),
+              dict(params=params(gpe, 1, (32, 32, 32), dt=5e-4), kind=gpe.REQ_EVOLVE, g=30., gd=5., tol=0.,
+                   check_every=50, max_steps=300)]
+    ids = [_submit(sv, others[0]), _submit(sv, others[1]), _submit(sv, target), _submit(sv, others[2])]
+    res = [sv.wait(i, timeout=120) for i in ids]
+    st = sv.stats()
+    sv.close()
+    assert all(r.status == 0 for r in res)
+    assert st["peak_active"] >= 2  # the target shared the GPU
+    assert _fields(res[2]) == _fields(alone)
+    assert res[0].steps == 400 and res[3].steps == 300
+
+
+def test_server_budget_and_refusal(gpe_lib):
+    gpe = gpe_lib
+    rq = _ground(gpe, (32, 32, 32), 50., 10.)
+    one = gpe.device_bytes(rq["params"])
+    sv = gpe.Server(int(one * 1.5))
+    ids = [_submit(sv, rq) for _ in range(3)]
+    big = dict(rq, params=params(gpe, 0, (64, 64, 64)))
+    ids.append(_submit(sv, big))
+    res = [sv.wait(i, timeout=120) for i in ids]
+    st = sv.stats()
+    sv.close()
+    assert [r.status for r in res[:3]] == [0, 0, 0]
+    assert res[3].status == 8  # GPE_ERR_BUDGET
+    assert st["peak_active"] == 1 and st["peak_bytes"] <= one * 1.5
+
+
+def test_server_ground_state_equals_chunked_run(gpe_lib):
+    gpe = gpe_lib
+    rq = _ground(gpe, (32, 32, 32), 80., 20.)
+    sv = gpe.Server(4 << 30)
+    r = sv.wait(_submit(sv, rq), timeout=120)
+    sv.close()
+    s = gpe.Solver(rq["params"])
+    s.init_gaussian()
+    s.calcnorm(True)
+    steps, mu_prev = 0, None
+    while True:
+        s.run(rq["check_every"], rq["g"], rq["gd"])
+        steps += rq["check_every"]
+        mu, en = s.calcmuen(rq["g"], rq["gd"])
+        if mu_prev is not None and abs(mu - mu_prev) < rq["tol"] * abs(mu):
+            break
+        mu_prev = mu
+        if steps >= rq["max_steps"]:
+            break
+    assert r.steps == steps and r.mu == mu and r.en == en
+    s.close()
