@@ -14,7 +14,9 @@ every 100 steps.  A "step" is one full split step over the 256^3 grid
          from page-locked host memory, K steps with rms every 100 steps,
          psi copied back, all inside the timed region
 --workload mixed512 measures the mixed-precision imaginary-time step at
-512x512x256 instead (FP32 / complex64 bulk, FP64 reductions and tables).
+512x512x256 instead (FP32 / complex64 bulk, FP64 reductions and tables);
+--workload batched64 the 64-instance mixed-precision batch (one CUDA graph per
+batch step); --workload serving the request server under Poisson arrivals.
 Multi-GPU (torchrun): independent replicas, one per GPU (weak scaling).
 --impl reference times the FP64 CPU restatement of the reference step
 (oracle/) on the host cores for the same workload.
@@ -50,7 +52,37 @@ WORKLOADS = {
                           "512x512x256, dx=0.25, dt=6.25e-3, trap (0.5,1,1.5), g=100, gd=30, R=32",
                      metric="grid-pt-steps/s (mixed-precision imaginary-time step, 512x512x256)",
                      b_min=8 * 4 + 8 * (129 / 256) * 8 + (129 / 256) * 8),
+    "batched64": dict(desc="64 independent imaginary-time solves, mixed precision, grids drawn from {48^3, 64^3, "
+                           "96x96x64, 128^3}, g~U[20,400], gd~U[0,0.9g], gamma,nu~U[0.5,2], lambda~U[0.5,8], "
+                           "dx~U[0.15,0.3], dt=0.1dx^2, R=half the shortest side (numpy PCG64 seed 20261203); one CUDA "
+                           "graph per batch step, autotuned tiles",
+                      metric="grid-pt-steps/s (64-instance mixed-precision batch)", dtype="f32 (FP64 reductions)",
+                      b_min=8 * 4 + 8 * (129 / 256) * 8 + (129 / 256) * 8),
+    "serving": dict(desc="request server: Poisson arrivals (numpy PCG64 seed 20261204), 50% ground states "
+                         "(imaginary time to |dmu/mu|<1e-8, checked every 100 steps, cap 4000) and 50% real-time runs "
+                         "(U{500..5000} steps), grids {48^3, 64^3, 128^3, 256^3}, parameters from the batch ranges, "
+                         "plain FP64, admission by a 150 GB HBM budget",
+                    metric="solves/s (request server, continuous batching)", dtype="f64"),
 }
+
+SERVING_UNIT = "solves/s"
+
+
+def draw_instances(n, seed, grids):
+    """n parameter sets in the C4 ranges from a seeded numpy generator."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        grid = grids[int(rng.integers(len(grids)))]
+        g = float(rng.uniform(20, 400))
+        gd = float(rng.uniform(0, 0.9 * g))
+        gam, nu = (float(v) for v in rng.uniform(0.5, 2.0, 2))
+        lam = float(rng.uniform(0.5, 8.0))
+        dx = float(rng.uniform(0.15, 0.3))
+        out.append(dict(grid=grid, g=g, gd=gd, trap=(gam, nu, lam), dx=dx, dt=0.1 * dx * dx,
+                        cutoff=0.5 * min(grid) * dx))
+    return out
 
 
 def load_peaks():
@@ -166,6 +198,190 @@ def traffic_table():
     return out
 
 
+def _clock_and_barrier(local):
+    import torch
+
+    def barrier():
+        torch.cuda.synchronize()
+    return ClockSampler(local), barrier
+
+
+def run_batched(args, wl):
+    """C4: 64 independent mixed-precision imaginary-time solves stepped as one
+    batch (one CUDA graph per batch step, tiles autotuned per grid)."""
+    import numpy as np
+    import torch
+    import gpe
+    K, W = args.steps, max(3, args.warmup)
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    inst = draw_instances(64, 20261203, [(48, 48, 48), (64, 64, 64), (96, 96, 64), (128, 128, 128)])
+
+    def make(prec):
+        ps = [gpe.make_params(gpe.MODE_IMAG, *d["grid"], d["dx"], d["dx"], d["dx"], d["dt"], *d["trap"], d["cutoff"],
+                              precision=prec, device=local) for d in inst]
+        b = gpe.Batch(ps, [d["g"] for d in inst], [d["gd"] for d in inst])
+        for i in range(len(inst)):
+            s = b.solver(i)
+            s.init_gaussian()
+            s.calcnorm(True)
+        return b
+
+    npts = sum(int(np.prod(d["grid"])) for d in inst)
+    b = make(gpe.PREC_MIXED)
+    t0 = time.perf_counter()
+    b.autotune(2)
+    tune_s = time.perf_counter() - t0
+    b.time_steps(W)
+    clocks, barrier = _clock_and_barrier(local)
+    n0 = b.launch_count()
+    barrier()
+    clocks.start()
+    ms = b.time_steps(K)
+    barrier()
+    clk = clocks.stop()
+    launches = b.launch_count() - n0
+    value = npts * K / (ms / 1e3)
+    # end to end: psi of every instance from page-locked host memory, K batch
+    # steps, psi back
+    host = [torch.empty(d["grid"], dtype=torch.float64).pin_memory() for d in inst]
+    for i, h in enumerate(host):
+        h.copy_(torch.from_numpy(b.solver(i).get_psi()))
+    barrier()
+    t0 = time.perf_counter()
+    for i, h in enumerate(host):
+        b.solver(i).set_psi_buffer(h.numpy())
+    b.run(K)
+    for i, h in enumerate(host):
+        b.solver(i).get_psi(h.numpy())
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    b.close()
+    # the same batch in plain FP64 (graph, default tiles), and the instances
+    # one after another in plain FP64 without a graph
+    b64 = make(gpe.PREC_FP64)
+    b64.time_steps(W)
+    ms64 = b64.time_steps(K)
+    b64.close()
+    seq_ms = 0.0
+    ks = max(5, K // 10)
+    for d in inst:
+        s = gpe.Solver(gpe.make_params(gpe.MODE_IMAG, *d["grid"], d["dx"], d["dx"], d["dx"], d["dt"], *d["trap"],
+                                       d["cutoff"], device=local))
+        s.init_gaussian()
+        s.time_steps(2, d["g"], d["gd"])
+        seq_ms += s.time_steps(ks, d["g"], d["gd"]) / ks
+        s.close()
+    seq_value = npts / (seq_ms / 1e3)
+    peak, peak_kind = load_peaks()
+    achieved = npts * K * wl["b_min"] / (ms / 1e3) / 1e9
+    cpu = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        oracle.build()
+        cores = os.cpu_count() or 1
+        oracle.set_threads(cores)
+        d = [x for x in inst if x["grid"] == (64, 64, 64)][0]
+        o = oracle.Oracle(0, 1, 64, 64, 64, d["dx"], d["dx"], d["dx"], d["dt"], *d["trap"], d["cutoff"])
+        o.init_gaussian()
+        o.run(1, d["g"], d["gd"])
+        t0 = time.perf_counter()
+        n = 0
+        while n < 20 and time.perf_counter() - t0 < 10:
+            o.run(1, d["g"], d["gd"])
+            n += 1
+        dt = time.perf_counter() - t0
+        o.close()
+        cpu = {"value": 64 ** 3 * n / dt, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": "%d FP64 steps of one 64^3 instance of the batch on the CPU restatement (OpenMP), %.1f s"
+                         % (n, dt)}
+    line = {"metric": wl["metric"], "value": value, "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": W,
+            "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": wl["dtype"], "data": "synthetic (seeded parameter draws, Gaussian initial states)",
+            "config": {"workload": wl["desc"], "instances": len(inst), "grid_points_per_batch_step": npts,
+                       "autotune_s": round(tune_s, 2),
+                       "batched_fp64_grid_pt_steps_per_s": npts * K / (ms64 / 1e3),
+                       "sequential_fp64_grid_pt_steps_per_s": seq_value,
+                       "speedup_vs_sequential_fp64": value / seq_value,
+                       "l2": "working set of the batch (about 1.3 GB) larger than L2, no flush"},
+            "roofline": {"bound": "hbm", "kernel": "whole batch step", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                         "bytes_per_point": wl["b_min"]},
+            "cpu_baseline": cpu,
+            "e2e": {"value": npts * K / e2e_s, "unit": UNIT, "h2d_bytes_per_step": npts * 8 / K,
+                    "d2h_bytes_per_step": npts * 8 / K,
+                    "note": "psi of all 64 instances H2D from page-locked memory, K batch steps, psi D2H, wall clock"},
+            "gpu_launches": launches, "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_serving(args, wl):
+    """C5: Poisson arrivals into the request server at several rates; p50 /
+    p99 latency and solves/s, against the same requests one at a time."""
+    import numpy as np
+    import torch
+    import gpe
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    nreq = max(8, min(args.steps, 24))
+    grids = [(48, 48, 48), (64, 64, 64), (128, 128, 128), (256, 256, 256)]
+    inst = draw_instances(nreq, 20261204, grids)
+    rng = np.random.default_rng(20261205)
+    reqs = []
+    for d in inst:
+        ground = bool(rng.integers(2) == 0)
+        steps = int(rng.integers(500, 5001))
+        p = gpe.make_params(gpe.MODE_IMAG if ground else gpe.MODE_REAL, *d["grid"], d["dx"], d["dx"], d["dx"],
+                            d["dt"] if ground else 0.1 * d["dt"], *d["trap"], d["cutoff"], device=local)
+        reqs.append(dict(p=p, kind=gpe.REQ_GROUND if ground else gpe.REQ_EVOLVE, g=d["g"], gd=d["gd"],
+                         tol=1e-8, check_every=100 if ground else 250, max_steps=4000 if ground else steps))
+    budget = 150 * 10 ** 9
+
+    def serve(rate, max_active):
+        sv = gpe.Server(budget, max_active=max_active, device=local)
+        arr = np.cumsum(np.random.default_rng(20261204 + int(rate)).exponential(1.0 / rate, len(reqs))) if rate else \
+            np.zeros(len(reqs))
+        t0 = time.perf_counter()
+        ids = []
+        for r, ta in zip(reqs, arr):
+            delay = ta - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            ids.append(sv.submit(r["p"], r["kind"], r["g"], r["gd"], r["tol"], r["check_every"], r["max_steps"]))
+        res = [sv.wait(i, timeout=600) for i in ids]
+        st = sv.stats()
+        sv.close()
+        lat = np.array([x.t_done - x.t_submit for x in res])
+        span = max(x.t_done for x in res) - min(x.t_submit for x in res)
+        return {"rate_req_per_s": rate, "solves_per_s": len(res) / span, "p50_s": float(np.percentile(lat, 50)),
+                "p99_s": float(np.percentile(lat, 99)), "peak_active": st["peak_active"],
+                "failed": int(sum(1 for x in res if x.status != 0)),
+                "steps": int(sum(x.steps for x in res))}
+
+    clocks, barrier = _clock_and_barrier(local)
+    clocks.start()
+    sweep = [serve(r, 64) for r in (20.0, 100.0, 500.0)]
+    clk = clocks.stop()
+    seq = serve(0.0, 1)  # one at a time: all queued at t = 0, one active solve
+    best = max(sweep, key=lambda x: x["solves_per_s"])
+    line = {"metric": wl["metric"], "value": sweep[-1]["solves_per_s"], "unit": SERVING_UNIT, "n_gpus": 1,
+            "steps": nreq, "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": wl["dtype"],
+            "data": "synthetic (seeded request draws and Poisson arrivals, Gaussian initial states)",
+            "config": {"workload": wl["desc"], "requests_per_rate": nreq, "hbm_budget_bytes": budget,
+                       "sweep": sweep, "one_at_a_time": seq,
+                       "speedup_vs_one_at_a_time": sweep[-1]["solves_per_s"] / seq["solves_per_s"],
+                       "p99_latency_s_at_500_req_per_s": sweep[-1]["p99_s"], "best_rate": best["rate_req_per_s"]},
+            "roofline": None, "cpu_baseline": None,
+            "e2e": {"value": sweep[-1]["solves_per_s"], "unit": SERVING_UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0, "note": "requests through the C ABI server; results read back per request"},
+            "gpu_launches": None, "clocks": clk}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -177,6 +393,14 @@ def main():
     args = ap.parse_args()
     K, W = args.steps, max(3, args.warmup)
     wl = WORKLOADS[args.workload]
+    if args.workload in ("batched64", "serving") and args.impl == "ours":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return 0
+        return run_batched(args, wl) if args.workload == "batched64" else run_serving(args, wl)
+    if "grid" not in wl:
+        print(json.dumps({"impl": "reference", "unavailable": "the CPU restatement times single solves; use the "
+                          "real256 or mixed512 workloads for the reference arm"}), flush=True)
+        return 0
     nx, ny, nz = wl["grid"]
     npts = nx * ny * nz
     cpu_steps = 3 if npts <= 256 ** 3 else 1

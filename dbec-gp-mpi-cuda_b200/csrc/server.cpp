@@ -6,12 +6,18 @@
 //      gpe_device_bytes of the active solves stays within the HBM budget and
 //      fewer than max_active are running (psi is created on the device and
 //      stays there until the request retires);
-//   2. queues one chunk of steps for every active solve, each on its own
-//      stream, so the solves run side by side on the GPU;
-//   3. waits for the chunks, checks convergence (ground state: relative change
-//      of mu between checks below tol; evolution: all steps done) and retires
-//      finished solves, freeing their memory for the next admissions.
-// Requests arriving while others run are admitted at the next chunk boundary.
+//   2. queues the next chunk of steps (plus, for a ground state, its mu) for
+//      active solves that have none in flight, in order of least remaining
+//      work (grid points x steps left), as long as the grid points of the
+//      chunks in flight stay within kFillPoints (the first always goes), each
+//      solve on its own stream with an event recorded behind it: the solves
+//      run side by side on the GPU, each at its own pace, and short requests
+//      are not held behind long ones;
+//   3. polls the chunks' events; for every finished chunk it checks
+//      convergence (ground state: relative change of mu between checks below
+//      tol; evolution: all steps done) and retires finished solves, freeing
+//      their memory for the next admissions.
+// Requests arriving while others run are admitted on the next turn.
 // A solve's arithmetic does not depend on what else is running: every solve
 // has its own handle, stream and buffers, and its chunk boundaries depend only
 // on its own request.
@@ -45,7 +51,16 @@ struct Active {
    double t_submit = 0., t_start = 0.;
    gpe_status st = GPE_OK;
    bool done = false;
+   bool inflight = false;
+   cudaEvent_t ev = nullptr;
+   cudaStream_t stream = nullptr;  // created by the server with a priority
 };
+
+// Grid points of the chunks kept in flight at once: about two 256^3 solves,
+// more than enough to fill the GPU, so admitting more only shares it.
+constexpr long long kFillPoints = 2LL * 256 * 256 * 256;
+
+long long npts_of(const gpe_request &rq) { return (long long) rq.p.nx * rq.p.ny * rq.p.nz; }
 
 struct Pending {
    long long id;
@@ -93,6 +108,10 @@ struct gpe_server {
       }
       gpe_destroy(a.s);
       a.s = nullptr;
+      if (a.ev) cudaEventDestroy(a.ev);
+      a.ev = nullptr;
+      if (a.stream) cudaStreamDestroy(a.stream);
+      a.stream = nullptr;
       r.t_done = now();
       std::lock_guard<std::mutex> lk(mu);
       results[a.id] = r;
@@ -106,8 +125,16 @@ struct gpe_server {
       return std::max(0L, std::min(a.rq.check_every, left));
    }
 
+   int prio_lo = 0, prio_mid = 0, prio_hi = 0;
+
    void run() {
       cudaSetDevice(device);
+      int least = 0, greatest = 0;
+      if (cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess) {
+         prio_lo = least;
+         prio_hi = greatest;
+         prio_mid = (least + greatest) / 2;
+      }
       std::vector<Active> active;
       long long used = 0;
       for (;;) {
@@ -140,7 +167,15 @@ struct gpe_server {
             if (a.bytes > budget) {
                a.st = sfail(GPE_ERR_BUDGET, "request exceeds the server's HBM budget");
             } else {
-               a.st = gpe_create(&a.rq.p, nullptr, &a.s);
+               // smaller solves on higher-priority streams: when the GPU is
+               // shared, the CTA scheduler serves them first, so short requests
+               // are not held back by long ones (shortest work first)
+               const long long npts = a.rq.p.nx * a.rq.p.ny * a.rq.p.nz;
+               const int pr = npts <= 64 * 64 * 64 ? prio_hi : (npts <= 128 * 128 * 128 ? prio_mid : prio_lo);
+               if (cudaStreamCreateWithPriority(&a.stream, cudaStreamNonBlocking, pr) != cudaSuccess)
+                  a.st = sfail(GPE_ERR_CUDA, "server: stream creation failed");
+               else
+                  a.st = gpe_create(&a.rq.p, a.stream, &a.s);
                if (a.st == GPE_OK) a.st = gpe_init_gaussian(a.s);
                if (a.st == GPE_OK && a.rq.kind == GPE_REQ_GROUND) {
                   double nrm;
@@ -152,6 +187,7 @@ struct gpe_server {
                   gpe_destroy(a.s);
                   a.s = nullptr;
                }
+               if (a.stream) cudaStreamDestroy(a.stream);
                gpe_result r{};
                r.id = a.id;
                r.status = a.st;
@@ -173,38 +209,73 @@ struct gpe_server {
             stats[2] = std::max(stats[2], (double) used);
          }
          if (active.empty()) continue;
-         // 2. one chunk per active solve, all queued before any wait
-         for (Active &a : active) {
+         // 2. next chunks, least remaining work first, within the fill budget
+         long long fill = 0;
+         for (const Active &a : active)
+            if (a.inflight) fill += npts_of(a.rq);
+         std::vector<Active *> order;
+         for (Active &a : active)
+            if (!a.inflight && !a.done) order.push_back(&a);
+         std::sort(order.begin(), order.end(), [](const Active *x, const Active *y) {
+            return npts_of(x->rq) * (x->rq.max_steps - x->steps) < npts_of(y->rq) * (y->rq.max_steps - y->steps);
+         });
+         for (Active *ap : order) {
+            Active &a = *ap;
+            if (fill > 0 && fill + npts_of(a.rq) > kFillPoints) continue;
+            fill += npts_of(a.rq);
+            if (!a.ev && cudaEventCreateWithFlags(&a.ev, cudaEventDisableTiming) != cudaSuccess) {
+               a.st = sfail(GPE_ERR_CUDA, "server: event creation failed");
+               a.done = true;
+               continue;
+            }
             const long n = chunk(a);
             a.st = gpe::queue_steps(a.s, n, a.rq.g, a.rq.gd);
             if (a.st == GPE_OK) a.st = gpe::queue_finish(a.s);
             if (a.st == GPE_OK && a.rq.kind == GPE_REQ_GROUND) a.st = gpe::queue_muen(a.s, a.rq.g, a.rq.gd);
+            if (a.st == GPE_OK && cudaEventRecord(a.ev, gpe::stream_of(a.s)) != cudaSuccess)
+               a.st = sfail(GPE_ERR_CUDA, "server: event record failed");
             a.steps += n;
-         }
-         {
+            if (a.st != GPE_OK) {
+               a.done = true;
+               continue;
+            }
+            a.inflight = true;
             std::lock_guard<std::mutex> lk(mu);
             stats[3] += 1;
          }
-         // 3. wait, check, retire
+         // 3. finished chunks: check, retire
+         bool progressed = false;
          for (Active &a : active) {
-            if (a.st == GPE_OK && a.rq.kind == GPE_REQ_GROUND) {
+            if (!a.inflight) continue;
+            const cudaError_t q = cudaEventQuery(a.ev);
+            if (q == cudaErrorNotReady) continue;
+            a.inflight = false;
+            progressed = true;
+            if (q != cudaSuccess) {
+               a.st = sfail(GPE_ERR_CUDA, cudaGetErrorString(q));
+               a.done = true;
+               continue;
+            }
+            if (a.rq.kind == GPE_REQ_GROUND) {
                double m = NAN, e = NAN;
                a.st = gpe::read_muen(a.s, &m, &e);
                if (a.st == GPE_OK && std::isfinite(a.mu_prev) && std::fabs(m - a.mu_prev) < a.rq.tol * std::fabs(m))
                   a.done = true;
                a.mu_prev = m;
-            } else if (a.st == GPE_OK) {
+            } else {
                a.st = gpe_synchronize(a.s);
             }
             if (a.steps >= a.rq.max_steps || a.st != GPE_OK) a.done = true;
          }
          for (Active &a : active)
-            if (a.done) {
+            if (a.done && !a.inflight) {
                used -= a.bytes;
                finish(a);
             }
-         active.erase(std::remove_if(active.begin(), active.end(), [](const Active &a) { return a.done; }),
+         active.erase(std::remove_if(active.begin(), active.end(),
+                                     [](const Active &a) { return a.done && !a.inflight && !a.s; }),
                       active.end());
+         if (!progressed) std::this_thread::sleep_for(std::chrono::microseconds(50));
       }
    }
 };
