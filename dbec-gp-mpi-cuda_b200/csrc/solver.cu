@@ -96,6 +96,7 @@ struct gpe_solver {
       void *M = nullptr, *N = nullptr;
    } sw[3];
    double *wz = nullptr;      // Simpson weights along z (norm partials)
+   double *wz2 = nullptr;     // wz[k] * z[k]^2 (rms partials)
    int nsm = 148;             // streaming multiprocessors of the device
    uint32_t *err = nullptr;   // device status word (bounded waits)
    // per-kernel profiling: when prof_ev is set, mark() records an event
@@ -376,7 +377,7 @@ static gpe_status plan_tiles(gpe_solver *s) {
             fixed = 128 + blk;
          } else {
             stage = ((size_t) TW * (d.nz + 16 / esz) * esz + 127) & ~(size_t) 127;
-            fixed = 128 + blk + (size_t) P * TW * sizeof(double);
+            fixed = 128 + blk + 2 * (size_t) P * TW * sizeof(double);
          }
       };
       int pick = 0;
@@ -471,6 +472,13 @@ static gpe_status setup_static(gpe_solver *s) {
    void *t = nullptr;
    CKS(upload(&t, wz.data(), wz.size()));
    s->wz = (double *) t;
+   std::vector<double> wz2(d.nz);
+   for (int k = 0; k < N; k++) {
+      const double z = (k - d.nz / 2) * s->p.dz;  // the mesh of initpsi
+      wz2[k] = wz[k] * (z * z);
+   }
+   CKS(upload(&t, wz2.data(), wz2.size()));
+   s->wz2 = (double *) t;
    CK(cudaMalloc(&s->err, sizeof(uint32_t)));
    CK(cudaMemset(s->err, 0, sizeof(uint32_t)));
    return GPE_OK;
@@ -517,6 +525,7 @@ static void free_all(gpe_solver *s) {
       if (s->sw[a].N) cudaFree(s->sw[a].N);
    }
    if (s->wz) cudaFree(s->wz);
+   if (s->wz2) cudaFree(s->wz2);
    if (s->err) cudaFree(s->err);
    if (s->own_stream && s->st) cudaStreamDestroy(s->st);
 }
@@ -747,35 +756,34 @@ template <class R, bool CPLX> struct Impl {
 
    static gpe_status ysweep(gpe_solver *s) { return sweep_xy<1, false>(s, 0., 0.); }
 
-   template <bool SIMP, int MSEG, int S> static gpe_status sweep_z_launch(gpe_solver *s) {
+   template <int MOM, int MSEG, int S> static gpe_status sweep_z_launch(gpe_solver *s) {
       auto &w = s->sw[2];
       const Dims &d = s->d;
-      const void *f = (const void *) k_sweep_z<R, CPLX, SIMP, MSEG, S>;
+      const void *f = (const void *) k_sweep_z<R, CPLX, MOM, MSEG, S>;
       CKS(smem_attr(f, w.smem));
       const long long ntiles = (d.nxy + w.TW - 1) / w.TW;
       const unsigned grid = (unsigned) std::min<long long>(ntiles, (long long) w.ctas * s->nsm);
-      k_sweep_z<R, CPLX, SIMP, MSEG, S><<<grid, ((w.TW * w.tab.P + 31) & ~31), w.smem, s->st>>>(
-          (P *) s->psi, d, w.tab, w.TW, w.LS, s->wz, s->p.dz / 3., s->rowA, s->err);
+      k_sweep_z<R, CPLX, MOM, MSEG, S><<<grid, ((w.TW * w.tab.P + 31) & ~31), w.smem, s->st>>>(
+          (P *) s->psi, d, w.tab, w.TW, w.LS, s->wz, s->wz2, s->p.dz / 3., s->rowA, s->rowB, s->err);
       CKL();
       mark(s);
       s->launches++;
       return GPE_OK;
    }
 
-   // z sweep; with simp each row also yields its Simpson integral of |psi|^2
-   static gpe_status zsweep(gpe_solver *s, bool simp) {
+   template <int MOM> static gpe_status zsweep_m(gpe_solver *s) {
       const auto &w = s->sw[2];
       if constexpr (kSeg32)
-         if (w.MSEG == 32) {
-            if (w.S == 3) return simp ? sweep_z_launch<true, 32, 3>(s) : sweep_z_launch<false, 32, 3>(s);
-            return simp ? sweep_z_launch<true, 32, 2>(s) : sweep_z_launch<false, 32, 2>(s);
-         }
-      if (w.MSEG == 8) {
-         if (w.S == 3) return simp ? sweep_z_launch<true, 8, 3>(s) : sweep_z_launch<false, 8, 3>(s);
-         return simp ? sweep_z_launch<true, 8, 2>(s) : sweep_z_launch<false, 8, 2>(s);
-      }
-      if (w.S == 3) return simp ? sweep_z_launch<true, 16, 3>(s) : sweep_z_launch<false, 16, 3>(s);
-      return simp ? sweep_z_launch<true, 16, 2>(s) : sweep_z_launch<false, 16, 2>(s);
+         if (w.MSEG == 32) return w.S == 3 ? sweep_z_launch<MOM, 32, 3>(s) : sweep_z_launch<MOM, 32, 2>(s);
+      if (w.MSEG == 8) return w.S == 3 ? sweep_z_launch<MOM, 8, 3>(s) : sweep_z_launch<MOM, 8, 2>(s);
+      return w.S == 3 ? sweep_z_launch<MOM, 16, 3>(s) : sweep_z_launch<MOM, 16, 2>(s);
+   }
+
+   // z sweep; mom 1: each row also yields its Simpson integral of |psi|^2
+   // (norm); mom 2: and of z^2 |psi|^2 (rms row partials)
+   static gpe_status zsweep(gpe_solver *s, int mom) {
+      if (mom == 2) return zsweep_m<2>(s);
+      return mom == 1 ? zsweep_m<1>(s) : zsweep_m<0>(s);
    }
 
    static gpe_status norm_final(gpe_solver *s, double *dev_out) {
@@ -817,10 +825,18 @@ template <class R, bool CPLX> struct Impl {
       k_rows_dens<R, CPLX><<<blocks_for(d.nxy, 128), 128, 0, s->st>>>((const P *) s->psi, d, s->p.dz, s->rowA, s->rowB,
                                                                      s->z2);
       CKL();
-      k_rms_final<<<1, 256, sizeof(double) * 3 * d.nx, s->st>>>(s->rowA, s->rowB, d, s->p.dx, s->p.dy, s->x2, s->y2,
-                                                                 dev_out);
+      s->launches++;
+      return rms_final(s, dev_out);
+   }
+
+   // rms from the row partials in rowA / rowB (k_rows_dens, or the z sweep
+   // of the step with mom = 2)
+   static gpe_status rms_final(gpe_solver *s, double *dev_out) {
+      const Dims &d = s->d;
+      k_rms_final<<<blocks_for(d.nx, kNormRowsPerCta), 32 * kNormRowsPerCta, 0, s->st>>>(
+          s->rowA, s->rowB, d, s->p.dx, s->p.dy, s->x2, s->y2, s->state, s->tmp, dev_out);
       CKL();
-      s->launches += 2;
+      s->launches++;
       return GPE_OK;
    }
 
@@ -841,12 +857,14 @@ template <class R, bool CPLX> struct Impl {
 
    // One split step (imag3d-mpicuda.cu:319-324): calcpsidd2, calcnu (fused
    // into the x sweep), x, y, z sweeps, and in imaginary time the norm.
-   static gpe_status step(gpe_solver *s, double g, double gd, double *dev_norm) {
+   // rms_rows: (real time) the z sweep also leaves the rms row partials of
+   // the new psi in rowA / rowB for rms_final.
+   static gpe_status step(gpe_solver *s, double g, double gd, double *dev_norm, bool rms_rows = false) {
       CKS(psidd2(s));
       CKS(xsweep(s, true, g, gd));
       CKS(ysweep(s));
       const bool imag = !CPLX;
-      CKS(zsweep(s, imag));
+      CKS(zsweep(s, imag ? 1 : (rms_rows ? 2 : 0)));
       if (imag) CKS(norm_final(s, dev_norm));
       return GPE_OK;
    }
@@ -1096,10 +1114,17 @@ extern "C" gpe_status gpe_run(gpe_solver *s, long nsteps, double *g, double *gd,
    for (long c = 0; c < nsteps && st == GPE_OK; c++) {
       *g += g_inc;
       *gd += gd_inc;
-      st = DISPATCH(s, step(s, *g, *gd, s->obs));
-      if (st == GPE_OK && rms_every > 0 && c % rms_every == 0) {
-         if (imag) st = DISPATCH(s, apply_scale(s));
-         if (st == GPE_OK) st = DISPATCH(s, rms(s, drms + 4 * (c / rms_every)));
+      const bool rms_here = rms_every > 0 && c % rms_every == 0;
+      // real time: the step's z sweep leaves the rms row partials (no extra
+      // pass over psi); imaginary time: renormalise first, then a full rms
+      st = DISPATCH(s, step(s, *g, *gd, s->obs, rms_here && !imag));
+      if (st == GPE_OK && rms_here) {
+         if (imag) {
+            st = DISPATCH(s, apply_scale(s));
+            if (st == GPE_OK) st = DISPATCH(s, rms(s, drms + 4 * (c / rms_every)));
+         } else {
+            st = DISPATCH(s, rms_final(s, drms + 4 * (c / rms_every)));
+         }
       }
    }
    if (st == GPE_OK && imag && nsteps > 0) st = DISPATCH(s, apply_scale(s));
@@ -1212,7 +1237,7 @@ extern "C" gpe_status gpe_calcluy(gpe_solver *s) {
 extern "C" gpe_status gpe_calcluz(gpe_solver *s) {
    CHECK_HANDLE(s);
    CK(cudaSetDevice(s->dev));
-   return DISPATCH(s, zsweep(s, false));
+   return DISPATCH(s, zsweep(s, 0));
 }
 
 extern "C" gpe_status gpe_synchronize(gpe_solver *s) {
@@ -1482,3 +1507,96 @@ int device_of(gpe_solver *s) { return s->dev; }
 long long kernels_per_step(gpe_solver *s) { return s->cplx ? 9 : 10; }
 
 }  // namespace gpe
+
+// --------------------------------------------------------------- snapshots
+namespace {
+struct SnapHeader {
+   char magic[8];           // "GPESNAP1"
+   uint32_t header_bytes;   // 192 (the header is zero-padded to that size)
+   uint32_t version;        // 1
+   gpe_params p;
+   double g, gd;
+   long long step;
+   unsigned long long payload_bytes;
+   unsigned long long fnv1a;
+};
+static_assert(sizeof(gpe_params) == 104, "gpe_params layout");
+constexpr size_t kSnapHeaderBytes = 192;
+static_assert(sizeof(SnapHeader) <= kSnapHeaderBytes, "snapshot header size");
+
+unsigned long long fnv1a(const unsigned char *p, size_t n) {
+   unsigned long long h = 1469598103934665603ULL;
+   for (size_t i = 0; i < n; i++) {
+      h ^= p[i];
+      h *= 1099511628211ULL;
+   }
+   return h;
+}
+}  // namespace
+
+extern "C" gpe_status gpe_snapshot_save(gpe_solver *s, const char *path, double g, double gd, long long step) {
+   CHECK_HANDLE(s);
+   if (!path) return fail(GPE_ERR_PARAM, "null path");
+   CK(cudaSetDevice(s->dev));
+   State st{};
+   CK(cudaMemcpyAsync(&st, s->state, sizeof(State), cudaMemcpyDeviceToHost, s->st));
+   CK(cudaStreamSynchronize(s->st));
+   if (st.scale != 1.) CKS(DISPATCH(s, apply_scale(s)));
+   const size_t nbytes = s->esz_psi * (size_t) s->d.npts;
+   std::vector<unsigned char> buf(kSnapHeaderBytes + nbytes, 0);
+   CK(cudaMemcpyAsync(buf.data() + kSnapHeaderBytes, s->psi, nbytes, cudaMemcpyDeviceToHost, s->st));
+   CK(cudaStreamSynchronize(s->st));
+   SnapHeader h{};
+   std::memcpy(h.magic, "GPESNAP1", 8);
+   h.header_bytes = (uint32_t) kSnapHeaderBytes;
+   h.version = 1;
+   h.p = s->p;
+   h.g = g;
+   h.gd = gd;
+   h.step = step;
+   h.payload_bytes = nbytes;
+   h.fnv1a = fnv1a(buf.data() + kSnapHeaderBytes, nbytes);
+   std::memcpy(buf.data(), &h, sizeof(h));
+   FILE *f = std::fopen(path, "wb");
+   if (!f) return fail(GPE_ERR_IO, std::string("cannot create ") + path);
+   const size_t w = std::fwrite(buf.data(), 1, buf.size(), f);
+   const int c = std::fclose(f);
+   if (w != buf.size() || c != 0) return fail(GPE_ERR_IO, std::string("short write to ") + path);
+   return GPE_OK;
+}
+
+extern "C" gpe_status gpe_snapshot_load(gpe_solver *s, const char *path, double *g, double *gd, long long *step) {
+   CHECK_HANDLE(s);
+   if (!path) return fail(GPE_ERR_PARAM, "null path");
+   FILE *f = std::fopen(path, "rb");
+   if (!f) return fail(GPE_ERR_IO, std::string("cannot open ") + path);
+   SnapHeader h{};
+   unsigned char hb[kSnapHeaderBytes];
+   const size_t r = std::fread(hb, 1, kSnapHeaderBytes, f);
+   std::memcpy(&h, hb, sizeof(h));
+   if (r != kSnapHeaderBytes || std::memcmp(h.magic, "GPESNAP1", 8) != 0 || h.version != 1 ||
+       h.header_bytes != kSnapHeaderBytes) {
+      std::fclose(f);
+      return fail(GPE_ERR_IO, std::string(path) + " is not a version-1 solver snapshot");
+   }
+   if (h.p.nx != s->p.nx || h.p.ny != s->p.ny || h.p.nz != s->p.nz || h.p.mode != s->p.mode ||
+       h.p.precision != s->p.precision) {
+      std::fclose(f);
+      return fail(GPE_ERR_PARAM, "snapshot grid, mode or precision differs from the handle's");
+   }
+   const size_t nbytes = s->esz_psi * (size_t) s->d.npts;
+   std::vector<unsigned char> buf(nbytes);
+   const size_t rp = h.payload_bytes == nbytes ? std::fread(buf.data(), 1, nbytes, f) : 0;
+   std::fclose(f);
+   if (rp != nbytes || fnv1a(buf.data(), nbytes) != h.fnv1a)
+      return fail(GPE_ERR_IO, std::string(path) + ": payload short or checksum mismatch");
+   CK(cudaSetDevice(s->dev));
+   CK(cudaMemcpyAsync(s->psi, buf.data(), nbytes, cudaMemcpyHostToDevice, s->st));
+   CK(cudaStreamSynchronize(s->st));
+   k_state_set<<<1, 1, 0, s->st>>>(s->state, 1.);
+   CKL();
+   if (g) *g = h.g;
+   if (gd) *gd = h.gd;
+   if (step) *step = h.step;
+   return GPE_OK;
+}

@@ -383,39 +383,59 @@ __global__ void k_state_set(State *st, double scale) {
    st->scale2 = scale * scale;
 }
 
-// rms sizes from per-row sums A = S_z |psi|^2, B = S_z z^2 |psi|^2
-// (calcrms, imag3d-mpicuda.cu:1639-1685).
-__global__ void k_rms_final(const double *__restrict__ rowA, const double *__restrict__ rowB, Dims d, double hx,
-                            double hy, const double *__restrict__ x2, const double *__restrict__ y2,
-                            double *__restrict__ out) {
-   extern __shared__ double sm[];
-   double *ta = sm, *tb = sm + d.nx, *tc = sm + 2 * d.nx;
-   for (int i = threadIdx.x; i < d.nx; i += blockDim.x) {
-      const double *ra = rowA + (long long) i * d.ny;
-      const double *rb = rowB + (long long) i * d.ny;
-      ta[i] = x2[i] * simpint_arr(hy, ra, d.ny);
-      tb[i] = simpint_arr(hy, rb, d.ny);
-      // y^2-weighted: Simpson of y2[j] * A[i][j] in the reference's order
-      double sumi = 0., sumj = 0., sumk = 0.;
-      const long N = d.ny;
-      for (long c = 1; c < N - 1; c += 2) {
-         sumi += y2[c] * ra[c];
-         sumj += y2[c - 1] * ra[c - 1];
-         sumk += y2[c + 1] * ra[c + 1];
+// calcrms (imag3d-mpicuda.cu:1639-1744) from the row partials rowA = S_z
+// |psi|^2 and rowB = S_z z^2 |psi|^2: <x^2> = S_x x^2 S_y rowA, <y^2> =
+// S_x S_y y^2 rowA, <z^2> = S_x S_y rowB; out = (r, rx, ry, rz).  Each warp
+// forms the three weighted Simpson sums over y of one x row into xs[3 nx];
+// the last CTA to finish integrates them over x.
+__global__ void __launch_bounds__(32 * kNormRowsPerCta) k_rms_final(const double *__restrict__ rowA,
+                                                                    const double *__restrict__ rowB, Dims d, double hx,
+                                                                    double hy, const double *__restrict__ x2,
+                                                                    const double *__restrict__ y2, State *st,
+                                                                    double *xs, double *__restrict__ out) {
+   const int lane = threadIdx.x & 31;
+   const int i = blockIdx.x * kNormRowsPerCta + (threadIdx.x >> 5);
+   if (i < d.nx) {
+      const double *ra = rowA + (long long) i * d.ny, *rb = rowB + (long long) i * d.ny;
+      double a = 0., b = 0., c = 0.;
+      for (int j = lane; j < d.ny; j += 32) {
+         const double w = simp_w(j, d.ny);
+         a = fma(w, ra[j], a);
+         b = fma(w, rb[j], b);
+         c = fma(w * y2[j], ra[j], c);
       }
-      double sum = sumj + 4. * sumi + sumk;
-      if (N % 2 == 0) sum += (5. * y2[N - 1] * ra[N - 1] + 8. * y2[N - 2] * ra[N - 2] - y2[N - 3] * ra[N - 3]) / 4.;
-      tc[i] = sum * hy / 3.;
+      for (int o = 16; o; o >>= 1) {
+         a += __shfl_xor_sync(0xffffffffu, a, o);
+         b += __shfl_xor_sync(0xffffffffu, b, o);
+         c += __shfl_xor_sync(0xffffffffu, c, o);
+      }
+      if (lane == 0) {
+         xs[i] = x2[i] * a * hy / 3.;
+         xs[d.nx + i] = c * hy / 3.;
+         xs[2 * d.nx + i] = b * hy / 3.;
+      }
    }
+   __threadfence();
    __syncthreads();
-   if (threadIdx.x == 0) {
-      const double rx = sqrt(simpint_arr(hx, ta, d.nx));
-      const double ry = sqrt(simpint_arr(hx, tc, d.nx));
-      const double rz = sqrt(simpint_arr(hx, tb, d.nx));
+   __shared__ bool last;
+   if (threadIdx.x == 0) last = atomicAdd(&st->ticket, 1u) == gridDim.x - 1;
+   __syncthreads();
+   if (!last || threadIdx.x >= 32) return;
+   __threadfence();
+   double m[3] = {0., 0., 0.};
+   for (int k = lane; k < d.nx; k += 32) {
+      const double w = simp_w(k, d.nx);
+      for (int q = 0; q < 3; q++) m[q] = fma(w, __ldcg(xs + q * d.nx + k), m[q]);
+   }
+   for (int q = 0; q < 3; q++)
+      for (int o = 16; o; o >>= 1) m[q] += __shfl_xor_sync(0xffffffffu, m[q], o);
+   if (lane == 0) {
+      const double rx = sqrt(m[0] * hx / 3.), ry = sqrt(m[1] * hx / 3.), rz = sqrt(m[2] * hx / 3.);
       out[1] = rx;
       out[2] = ry;
       out[3] = rz;
       out[0] = sqrt(rx * rx + ry * ry + rz * rz);
+      st->ticket = 0u;
    }
 }
 

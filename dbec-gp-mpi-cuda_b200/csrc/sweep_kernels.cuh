@@ -90,7 +90,8 @@ template <class R, bool CPLX> struct SegOps {
 // SPW = 32 / TW consecutive segments of each of its TW lines.  blk is a
 // shared scratch of 2 * (NW + 1) * TW elements (NW warps hold segments).
 // Writes the swept line back in place.  When simp_w is non-null, *simp
-// receives this thread's share of sum_i simp_w[i] |psi'_i|^2.
+// receives this thread's share of sum_i simp_w[i] |psi'_i|^2, and when
+// simp_w2 is non-null *simp2 that of sum_i simp_w2[i] |psi'_i|^2.
 //
 // Carries: segment p maps the value entering at its top (index hf+1) to the
 // value at its bottom (index lo) by the affine map x -> b + a x with
@@ -101,7 +102,8 @@ template <class R, bool CPLX> struct SegOps {
 template <class R, bool CPLX, int MSEG>
 __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, int cs, int c, int p, int TW,
                                           const SegTab &tb, typename Tr<R, CPLX>::P *blk, const double *simp_w,
-                                          double *simp) {
+                                          double *simp, const double *simp_w2 = nullptr,
+                                          double *simp2 = nullptr) {
    using Op = SegOps<R, CPLX>;
    using P = typename Tr<R, CPLX>::P;
    const int n = tb.n, m = tb.m, NP = tb.P;
@@ -196,7 +198,7 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
       bb[w * TW + c] = sb;
    }
    __syncthreads();
-   double acc = 0.;
+   double acc = 0., acc2 = 0.;
    {
       P x = zero_of<P>();  // psi' entering the first segment of this warp
       for (int ww = 0; ww < w; ww++) x = Op::fma_(ba[ww * TW + c], x, bb[ww * TW + c]);
@@ -210,7 +212,11 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
                const int k = lo + q + 1;
                const P val = Op::fma_(Op::ld(tb.N, k), fin, bt[q]);
                line[k * es] = val;
-               if (simp_w) acc += simp_w[k] * (double) dens2(val);
+               if (simp_w) {
+                  const double f = (double) dens2(val);
+                  acc += simp_w[k] * f;
+                  if (simp_w2) acc2 += simp_w2[k] * f;
+               }
             }
          }
          if (p == 0) line[0] = zero_of<P>();
@@ -218,6 +224,7 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
       }
    }
    if (simp) *simp = acc;
+   if (simp2) *simp2 = acc2;
 }
 
 // ---------------------------------------------------------------------------
@@ -335,13 +342,18 @@ __global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) k_sweep_xy(const 
 }
 
 // z sweep.  Tile: TR consecutive (x, y) rows, each copied by one bulk copy to
-// a padded shared row (stride LS elements).  With SIMP every row also yields
-// its Simpson integral of |psi'|^2 (simpint over z, diffint.cu:106) for the
-// norm of the step.
-template <class R, bool CPLX, bool SIMP, int MSEG, int S>
+// a padded shared row (stride LS elements).  With MOM >= 1 every row also
+// yields its Simpson integral of |psi'|^2 over z (simpint, diffint.cu:106),
+// for the norm of the step (rowsum); with MOM = 2 also that of z^2 |psi'|^2
+// (rowsum2), the row partials of calcrms, so an rms sample after the step
+// needs no extra pass over psi.
+template <class R, bool CPLX, int MOM, int MSEG, int S>
 __global__ void __launch_bounds__(256, kSweepCtas[0]) k_sweep_z(typename Tr<R, CPLX>::P *__restrict__ psi, Dims d, SegTab tb,
-                                                    int TR, int LS, const double *__restrict__ wz, double hz3,
-                                                    double *__restrict__ rowsum, uint32_t *err) {
+                                                    int TR, int LS, const double *__restrict__ wz,
+                                                    const double *__restrict__ wz2, double hz3,
+                                                    double *__restrict__ rowsum, double *__restrict__ rowsum2,
+                                                    uint32_t *err) {
+   constexpr bool SIMP = MOM >= 1;
    using P = typename Tr<R, CPLX>::P;
    extern __shared__ __align__(16) unsigned char smem_raw[];
    __shared__ __align__(8) uint64_t full[S];
@@ -353,6 +365,7 @@ __global__ void __launch_bounds__(256, kSweepCtas[0]) k_sweep_z(typename Tr<R, C
    const int NW = (tb.P + 32 / TR - 1) / (32 / TR);
    P *blk = (P *) (base + S * stage_bytes);
    double *part = (double *) (blk + 2 * (NW + 1) * TR);
+   double *part2 = part + tb.P * TR;
    const int ntiles = (int) ((d.nxy + TR - 1) / TR);
    auto nrows = [&](int t) -> int {
       const long long r0 = (long long) t * TR;
@@ -390,15 +403,22 @@ __global__ void __launch_bounds__(256, kSweepCtas[0]) k_sweep_z(typename Tr<R, C
          for (int e = threadIdx.x; e < (TR - nr) * LS; e += blockDim.x) tile[nr * LS + e] = zero_of<P>();
          __syncthreads();
       }
-      double my = 0.;
-      seg_sweep<R, CPLX, MSEG>(tile, 1, LS, c, p, TR, tb, blk, SIMP ? wz : nullptr, SIMP ? &my : nullptr);
+      double my = 0., my2 = 0.;
+      seg_sweep<R, CPLX, MSEG>(tile, 1, LS, c, p, TR, tb, blk, SIMP ? wz : nullptr, SIMP ? &my : nullptr,
+                               MOM == 2 ? wz2 : nullptr, MOM == 2 ? &my2 : nullptr);
       if (SIMP && p < tb.P) part[p * TR + c] = my;
+      if (MOM == 2 && p < tb.P) part2[p * TR + c] = my2;
       fence_proxy_async();
       __syncthreads();
       if (SIMP && p == 0 && c < nr) {
          double sum = 0.;
          for (int pp = 0; pp < tb.P; pp++) sum += part[pp * TR + c];
          rowsum[(long long) t * TR + c] = sum * hz3;
+         if (MOM == 2) {
+            double sum2 = 0.;
+            for (int pp = 0; pp < tb.P; pp++) sum2 += part2[pp * TR + c];
+            rowsum2[(long long) t * TR + c] = sum2 * hz3;
+         }
       }
       if (threadIdx.x == 0) copy_tile(t, q, false);
    }

@@ -92,6 +92,8 @@ _SIGS = {
     "gpe_step_kernel_name": (C.c_char_p, [_P, C.c_int]),
     "gpe_step_kernel_bytes": (C.c_double, [_P, C.c_int]),
     "gpe_norm_noalloc": (C.c_int, [_P, C.c_int, C.c_long, C.c_long, C.c_long, _D, _D, _D, _P, _P]),
+    "gpe_snapshot_save": (C.c_int, [_P, C.c_char_p, _D, _D, C.c_longlong]),
+    "gpe_snapshot_load": (C.c_int, [_P, C.c_char_p, _DP, _DP, C.POINTER(C.c_longlong)]),
     "gpe_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
     "gpe_set_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
     "gpe_autotune": (C.c_int, [_P, _D, _D, C.c_int, C.POINTER(Tuning)]),
@@ -295,6 +297,16 @@ class Solver:
         ms = C.c_double()
         _check(lib().gpe_time_steps(self.h, int(nsteps), float(g), float(gd), C.byref(ms)))
         return ms.value
+
+    # -- snapshots -----------------------------------------------------------
+    def snapshot_save(self, path, g=0.0, gd=0.0, step=0):
+        _check(lib().gpe_snapshot_save(self.h, os.fsencode(path), float(g), float(gd), int(step)))
+
+    def snapshot_load(self, path):
+        """Returns (g, gd, step) stored with the snapshot."""
+        g, gd, st = C.c_double(), C.c_double(), C.c_longlong()
+        _check(lib().gpe_snapshot_load(self.h, os.fsencode(path), C.byref(g), C.byref(gd), C.byref(st)))
+        return g.value, gd.value, st.value
 
     # -- tile configuration --------------------------------------------------
     def get_tuning(self) -> Tuning:

@@ -156,6 +156,19 @@ gpe_status gpe_set_tuning(gpe_solver *s, const gpe_tuning *t);
  * configuration is applied and returned in *best (may be NULL). */
 gpe_status gpe_autotune(gpe_solver *s, double g, double gd, int nsteps, gpe_tuning *best);
 
+/* Snapshot of a solve (no reference counterpart: the reference's
+ * imag3d-den.bin keeps sqrt(density) only and loses the phase).  The file
+ * holds a 192-byte header (magic "GPESNAP1", format version 1, the handle's
+ * gpe_params, couplings g and gd, the caller's step counter, payload size
+ * and a 64-bit FNV-1a checksum of the payload) followed by psi exactly as the
+ * handle stores it (FP64 or FP32, real or interleaved complex, x-major).  A
+ * pending imaginary-time renormalisation is applied before writing. */
+gpe_status gpe_snapshot_save(gpe_solver *s, const char *path, double g, double gd, long long step);
+/* Loads a snapshot into a handle with the same grid, mode and precision
+ * (GPE_ERR_PARAM otherwise; GPE_ERR_IO for a short, corrupt or foreign file);
+ * returns the stored couplings and step counter (pointers may be NULL). */
+gpe_status gpe_snapshot_load(gpe_solver *s, const char *path, double *g, double *gd, long long *step);
+
 /* ---------------------------------------------------------------- batch
  * Many independent solves with their own grids and parameters (no reference
  * counterpart: the reference runs one solve per MPI job).  Each instance is a
