@@ -165,7 +165,7 @@ __device__ __forceinline__ void fft_stage_ip(C *buf, int n, int Ns, unsigned mag
 
 // Full in-place transform of L interleaved lines in buf (PPT as above).
 template <int L, class C, bool INV, int PPT>
-__device__ void fft_lines_ip(C *buf, const FftPlan &pl, const C *tw, int twmul) {
+__device__ __forceinline__ void fft_lines_ip(C *buf, const FftPlan &pl, const C *tw, int twmul) {
    // make_plan orders the stages by radix (8, 4, 2, 3, 5): one loop per radix
    // (a switch over the radix inside one loop made ptxas spill the values
    // held across the barriers)
