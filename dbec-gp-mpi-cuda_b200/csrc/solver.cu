@@ -720,20 +720,29 @@ template <class R, bool CPLX> struct Impl {
       return GPE_OK;
    }
 
-   template <int AXIS, bool NU, int MSEG, int S> static gpe_status sweep_xy_launch(gpe_solver *s, double g, double gd) {
+   template <int AXIS, bool NU, int MSEG, int S, int TWC> static gpe_status sweep_xy_launch_t(gpe_solver *s, double g, double gd) {
       auto &w = s->sw[AXIS];
       const Dims &d = s->d;
-      const void *f = (const void *) k_sweep_xy<R, CPLX, AXIS, NU, MSEG, S>;
+      const void *f = (const void *) k_sweep_xy<R, CPLX, AXIS, NU, MSEG, S, TWC>;
       CKS(smem_attr(f, w.smem));
       const int nzb = (d.nz + w.TW - 1) / w.TW;
       const int ntiles = (AXIS == 0 ? d.ny : d.nx) * nzb;
       const unsigned grid = (unsigned) std::min(ntiles, w.ctas * s->nsm);
-      k_sweep_xy<R, CPLX, AXIS, NU, MSEG, S><<<grid, ((w.TW * w.tab.P + 31) & ~31), w.smem, s->st>>>(
+      k_sweep_xy<R, CPLX, AXIS, NU, MSEG, S, TWC><<<grid, ((w.TW * w.tab.P + 31) & ~31), w.smem, s->st>>>(
           w.tm_psi, w.tm_phi, d, w.tab, trap_of(s), g, gd, s->p.dt, s->state, w.TW, w.boxn, w.nbox, s->err);
       CKL();
       mark(s);
       s->launches++;
       return GPE_OK;
+   }
+
+   // FP64 tiles of 8 or 16 lines use kernels compiled for that width
+   template <int AXIS, bool NU, int MSEG, int S> static gpe_status sweep_xy_launch(gpe_solver *s, double g, double gd) {
+      if constexpr (std::is_same<R, double>::value) {
+         if (s->sw[AXIS].TW == 8) return sweep_xy_launch_t<AXIS, NU, MSEG, S, 8>(s, g, gd);
+         if (s->sw[AXIS].TW == 16) return sweep_xy_launch_t<AXIS, NU, MSEG, S, 16>(s, g, gd);
+      }
+      return sweep_xy_launch_t<AXIS, NU, MSEG, S, 0>(s, g, gd);
    }
 
    // 32-point segments exist for FP32 real lines only (register budget)
@@ -756,19 +765,27 @@ template <class R, bool CPLX> struct Impl {
 
    static gpe_status ysweep(gpe_solver *s) { return sweep_xy<1, false>(s, 0., 0.); }
 
-   template <int MOM, int MSEG, int S> static gpe_status sweep_z_launch(gpe_solver *s) {
+   template <int MOM, int MSEG, int S, int TWC> static gpe_status sweep_z_launch_t(gpe_solver *s) {
       auto &w = s->sw[2];
       const Dims &d = s->d;
-      const void *f = (const void *) k_sweep_z<R, CPLX, MOM, MSEG, S>;
+      const void *f = (const void *) k_sweep_z<R, CPLX, MOM, MSEG, S, TWC>;
       CKS(smem_attr(f, w.smem));
       const long long ntiles = (d.nxy + w.TW - 1) / w.TW;
       const unsigned grid = (unsigned) std::min<long long>(ntiles, (long long) w.ctas * s->nsm);
-      k_sweep_z<R, CPLX, MOM, MSEG, S><<<grid, ((w.TW * w.tab.P + 31) & ~31), w.smem, s->st>>>(
+      k_sweep_z<R, CPLX, MOM, MSEG, S, TWC><<<grid, ((w.TW * w.tab.P + 31) & ~31), w.smem, s->st>>>(
           (P *) s->psi, d, w.tab, w.TW, w.LS, s->wz, s->wz2, s->p.dz / 3., s->rowA, s->rowB, s->err);
       CKL();
       mark(s);
       s->launches++;
       return GPE_OK;
+   }
+
+   template <int MOM, int MSEG, int S> static gpe_status sweep_z_launch(gpe_solver *s) {
+      if constexpr (std::is_same<R, double>::value) {
+         if (s->sw[2].TW == 8) return sweep_z_launch_t<MOM, MSEG, S, 8>(s);
+         if (s->sw[2].TW == 16) return sweep_z_launch_t<MOM, MSEG, S, 16>(s);
+      }
+      return sweep_z_launch_t<MOM, MSEG, S, 0>(s);
    }
 
    template <int MOM> static gpe_status zsweep_m(gpe_solver *s) {

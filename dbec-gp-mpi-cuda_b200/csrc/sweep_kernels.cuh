@@ -99,13 +99,14 @@ template <class R, bool CPLX> struct SegOps {
 // of the maps of all segments above it: a suffix scan, done with shuffles
 // inside a warp and a short chain over the warps above.  The forward
 // recurrence composes x -> psi'~[hf+1] + N[hf+1] x from the bottom (prefix).
-template <class R, bool CPLX, int MSEG>
-__device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, int cs, int c, int p, int TW,
+template <class R, bool CPLX, int MSEG, int TWC = 0>
+__device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, int cs, int c, int p, int tw_arg,
                                           const SegTab &tb, typename Tr<R, CPLX>::P *blk, const double *simp_w,
                                           double *simp, const double *simp_w2 = nullptr,
                                           double *simp2 = nullptr) {
    using Op = SegOps<R, CPLX>;
    using P = typename Tr<R, CPLX>::P;
+   const int TW = TWC > 0 ? TWC : tw_arg;  // lines per CTA (compile time when TWC > 0)
    const int n = tb.n, m = tb.m, NP = tb.P;
    const int SPW = 32 / TW;              // segments of one line inside a warp
    const int NW = (NP + SPW - 1) / SPW;  // warps that hold segments
@@ -250,13 +251,14 @@ template <int S> __device__ __forceinline__ void wait_stage_free() {
 // (y sweep) plane, the whole line along the swept axis, brought in by TMA.
 // With NU the x sweep first applies the pending 1/norm and calcnu to the tile
 // (needs phi).
-template <class R, bool CPLX, int AXIS, bool NU, int MSEG, int S>
+template <class R, bool CPLX, int AXIS, bool NU, int MSEG, int S, int TWC>
 __global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) k_sweep_xy(const __grid_constant__ CUtensorMap tm_psi,
                                                      const __grid_constant__ CUtensorMap tm_phi, Dims d, SegTab tb,
                                                      Trap trap, double g, double gd, double dt,
-                                                     const State *__restrict__ st, int TW, int boxn, int nbox,
+                                                     const State *__restrict__ st, int tw_arg, int boxn, int nbox,
                                                      uint32_t *err) {
    using P = typename Tr<R, CPLX>::P;
+   const int TW = TWC > 0 ? TWC : tw_arg;
    extern __shared__ __align__(16) unsigned char smem_raw[];
    __shared__ __align__(8) uint64_t full[S];
    const int n = tb.n;
@@ -333,7 +335,7 @@ __global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) k_sweep_xy(const 
          }
          __syncthreads();
       }
-      seg_sweep<R, CPLX, MSEG>(tile, TW, 1, c, p, TW, tb, blk, nullptr, nullptr);
+      seg_sweep<R, CPLX, MSEG, TWC>(tile, TW, 1, c, p, TW, tb, blk, nullptr, nullptr);
       fence_proxy_async();
       __syncthreads();
       if (threadIdx.x == 0) copy_tile(t, q, false);
@@ -347,13 +349,14 @@ __global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) k_sweep_xy(const 
 // for the norm of the step (rowsum); with MOM = 2 also that of z^2 |psi'|^2
 // (rowsum2), the row partials of calcrms, so an rms sample after the step
 // needs no extra pass over psi.
-template <class R, bool CPLX, int MOM, int MSEG, int S>
+template <class R, bool CPLX, int MOM, int MSEG, int S, int TWC>
 __global__ void __launch_bounds__(256, kSweepCtas[0]) k_sweep_z(typename Tr<R, CPLX>::P *__restrict__ psi, Dims d, SegTab tb,
-                                                    int TR, int LS, const double *__restrict__ wz,
+                                                    int tr_arg, int LS, const double *__restrict__ wz,
                                                     const double *__restrict__ wz2, double hz3,
                                                     double *__restrict__ rowsum, double *__restrict__ rowsum2,
                                                     uint32_t *err) {
    constexpr bool SIMP = MOM >= 1;
+   const int TR = TWC > 0 ? TWC : tr_arg;
    using P = typename Tr<R, CPLX>::P;
    extern __shared__ __align__(16) unsigned char smem_raw[];
    __shared__ __align__(8) uint64_t full[S];
@@ -404,7 +407,7 @@ __global__ void __launch_bounds__(256, kSweepCtas[0]) k_sweep_z(typename Tr<R, C
          __syncthreads();
       }
       double my = 0., my2 = 0.;
-      seg_sweep<R, CPLX, MSEG>(tile, 1, LS, c, p, TR, tb, blk, SIMP ? wz : nullptr, SIMP ? &my : nullptr,
+      seg_sweep<R, CPLX, MSEG, TWC>(tile, 1, LS, c, p, TR, tb, blk, SIMP ? wz : nullptr, SIMP ? &my : nullptr,
                                MOM == 2 ? wz2 : nullptr, MOM == 2 ? &my2 : nullptr);
       if (SIMP && p < tb.P) part[p * TR + c] = my;
       if (MOM == 2 && p < tb.P) part2[p * TR + c] = my2;
