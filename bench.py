@@ -198,6 +198,20 @@ def traffic_table():
     return out
 
 
+def replica_throughput(local_ms, units_per_rank, dist=None, device=None):
+    """Whole-job throughput of independent replicas: every rank processed
+    units_per_rank units in local_ms; the job takes as long as its slowest
+    rank (max over ranks).  Returns (units per second of all ranks together,
+    the max-over-ranks milliseconds)."""
+    import torch
+    world = dist.get_world_size() if dist is not None else 1
+    t = torch.tensor([float(local_ms)], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    return units_per_rank * world / (ms_max / 1e3), ms_max
+
+
 def _clock_and_barrier(local):
     import torch
 
@@ -456,11 +470,7 @@ def main():
     barrier()
     clk = clocks.stop()
     launches = s.launch_count() - n0
-    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    value = npts * K * world / (ms_max / 1e3)
+    value, ms_max = replica_throughput(ms, npts * K, dist, device="cuda")
 
     # per-kernel durations (CUDA events around each launch of a few steps) and
     # the roofline of the dominant kernel
@@ -494,10 +504,7 @@ def main():
     s.get_psi(host_out.numpy())
     barrier()
     e2e_s = time.perf_counter() - t0
-    e_t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(e_t, op=dist.ReduceOp.MAX)
-    e2e_value = npts * K * world / float(e_t.item())
+    e2e_value, _ = replica_throughput(e2e_s * 1e3, npts * K, dist, device="cuda")
     bytes_psi = npts * wl["psi_bytes"]
     e2e = {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": bytes_psi / K,
            "d2h_bytes_per_step": (bytes_psi + rms.size * 8) / K,

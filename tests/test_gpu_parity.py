@@ -205,3 +205,34 @@ def test_cli_golden_chain(tmp_path):
     assert dyna.shape == gd.shape
     ulp = 10.0 ** (np.floor(np.log10(np.maximum(np.abs(gd), 1e-300))) - 6)
     assert np.all((np.abs(dyna - gd) <= 0.6 * ulp) | (gd == 0))
+
+
+EDGE_SHAPES = [(18, 10, 20),     # nx*ny not a multiple of the 8-row tiles (partial tiles)
+               (320, 10, 12),    # x lines longer than one 256-row TMA box (two boxes)
+               (12, 1024, 8),    # longest y lines: narrowest FFT tiles
+               (8, 10, 1024)]    # longest z rows: 16 points per thread in the z passes
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("shape", EDGE_SHAPES)
+def test_operators_edge_shapes(gpe_lib, oracle_mod, mode, shape):
+    s, o = make_pair(gpe_lib, oracle_mod, mode, shape, spacing=(.3, .2, .25))
+    psi = seeded_psi(shape, mode, seed=5)
+    s.set_psi(psi)
+    o.set_psi(psi)
+    s.calcpsidd2()
+    o.calcpsidd2()
+    assert rel(s.get_phi(), o.get_phi()) <= OP_TOL
+    s.calcnu(21.0, 7.0)
+    o.calcnu(21.0, 7.0)
+    for name in ("calclux", "calcluy", "calcluz"):
+        getattr(s, name)()
+        getattr(o, name)()
+        assert rel(s.get_psi(), o.get_psi()) <= OP_TOL, name
+    rs = s.run(3, 21.0, 7.0)
+    ro = o.run(3, 21.0, 7.0)
+    assert rel(s.get_psi(), o.get_psi()) <= OP_TOL
+    if mode == 0:
+        assert abs(rs[2] / ro[2] - 1) <= OP_TOL
+    assert rel(s.calcrms(), o.calcrms()) <= OP_TOL
+    s.close()
