@@ -53,6 +53,48 @@ struct Trap {
    }
 };
 
+// Separable trap factors of calcnu in imaginary time.  V = 0.5 par (g2 x^2 +
+// n2 y^2 + l2 z^2) is a sum over the axes, so exp(-dt V) is a product of one
+// factor per axis; the factors are tabulated per axis on the host (long
+// double) and only the nonlinear part of the exponent is evaluated per point.
+struct LinPhase {
+   const void *ex, *ey, *ez;
+};
+
+// exp(t) for the nonlinear part of the step's exponent, which is small in
+// practice: Taylor series on |t| <= 0.5 (through t^16; the first omitted term
+// is below 2.2e-20 relative), the library function beyond.
+__device__ __forceinline__ double exp_small(double t) {
+   if (fabs(t) > 0.5) return exp(t);
+   constexpr double f2 = 1. / 2, f3 = f2 / 3, f4 = f3 / 4, f5 = f4 / 5, f6 = f5 / 6, f7 = f6 / 7, f8 = f7 / 8,
+                    f9 = f8 / 9, f10 = f9 / 10, f11 = f10 / 11, f12 = f11 / 12, f13 = f12 / 13, f14 = f13 / 14,
+                    f15 = f14 / 15, f16 = f15 / 16;
+   double e = f16;
+   e = fma(e, t, f15);
+   e = fma(e, t, f14);
+   e = fma(e, t, f13);
+   e = fma(e, t, f12);
+   e = fma(e, t, f11);
+   e = fma(e, t, f10);
+   e = fma(e, t, f9);
+   e = fma(e, t, f8);
+   e = fma(e, t, f7);
+   e = fma(e, t, f6);
+   e = fma(e, t, f5);
+   e = fma(e, t, f4);
+   e = fma(e, t, f3);
+   e = fma(e, t, f2);
+   e = fma(e, t, 1.);
+   return fma(e, t, 1.);
+}
+
+// calcnu of one FP64 element with the trap factor lin = exp(-dt V) from the
+// axis tables: the same step as nu_op up to rounding.
+__device__ __forceinline__ double nu_split(double p, double phi, double lin, double g, double gd, double dt,
+                                           double invN) {
+   const double thn = dt * fma(p * p, g, (phi * invN) * gd);
+   return p * (lin * exp_small(-thn));
+}
 // calcnu on one element (imag3d-mpicuda.cu:1759-1783, real3d:1856-1883).
 template <class R>
 __device__ __forceinline__ R nu_op(R p, R phi, R V, R g, R gd, R dt, R invN) {

@@ -81,6 +81,7 @@ struct gpe_solver {
    void *alpha[3] = {nullptr, nullptr, nullptr}, *gamma[3] = {nullptr, nullptr, nullptr};
    double2 A[3], A0r[3], mA[3];
    double *x2 = nullptr, *y2 = nullptr, *z2 = nullptr;
+   void *lin[3] = {nullptr, nullptr, nullptr};  // per-axis trap factors of calcnu, imag (LinPhase)
    double *rowA = nullptr, *rowB = nullptr, *tmp = nullptr, *obs = nullptr;
    long long row_cap = 0;  // doubles in rowA / rowB: the largest of nx*ny, nx*nz, ny*nz
    State *state = nullptr;
@@ -525,6 +526,8 @@ static void free_all(gpe_solver *s) {
       if (s->sw[a].N) cudaFree(s->sw[a].N);
    }
    if (s->wz) cudaFree(s->wz);
+   for (void *q : s->lin)
+      if (q) cudaFree(q);
    if (s->wz2) cudaFree(s->wz2);
    if (s->err) cudaFree(s->err);
    if (s->own_stream && s->st) cudaStreamDestroy(s->st);
@@ -592,6 +595,19 @@ static gpe_status create_impl(const gpe_params *p, void *stream, gpe_solver *s) 
    CKS(upload(&t, s->hx2.data(), d.nx)); s->x2 = (double *) t;
    CKS(upload(&t, s->hy2.data(), d.ny)); s->y2 = (double *) t;
    CKS(upload(&t, s->hz2.data(), d.nz)); s->z2 = (double *) t;
+   // trap factors per axis for calcnu in imaginary time: exp(-dt 0.5 par c x^2)
+   if (!s->cplx) {
+      const long double hp = 0.5L * (long double) s->par, dt = (long double) p->dt;
+      const long double cf[3] = {(long double) p->gamma * p->gamma, (long double) p->nu * p->nu,
+                                 (long double) p->lambda * p->lambda};
+      const std::vector<double> *sq[3] = {&s->hx2, &s->hy2, &s->hz2};
+      for (int a = 0; a < 3; a++) {
+         const size_t n = sq[a]->size();
+         std::vector<double> tab(n);
+         for (size_t i = 0; i < n; i++) tab[i] = (double) expl(-dt * hp * cf[a] * (long double) (*sq[a])[i]);
+         CKS(upload(&s->lin[a], tab.data(), tab.size()));
+      }
+   }
    CK(cudaDeviceSynchronize());
    return GPE_OK;
 }
@@ -729,7 +745,8 @@ template <class R, bool CPLX> struct Impl {
       const int ntiles = (AXIS == 0 ? d.ny : d.nx) * nzb;
       const unsigned grid = (unsigned) std::min(ntiles, w.ctas * s->nsm);
       k_sweep_xy<R, CPLX, AXIS, NU, MSEG, S, TWC><<<grid, ((w.TW * w.tab.P + 31) & ~31), w.smem, s->st>>>(
-          w.tm_psi, w.tm_phi, d, w.tab, trap_of(s), g, gd, s->p.dt, s->state, w.TW, w.boxn, w.nbox, s->err);
+          w.tm_psi, w.tm_phi, d, w.tab, trap_of(s), LinPhase{s->lin[0], s->lin[1], s->lin[2]}, g, gd, s->p.dt,
+          s->state, w.TW, w.boxn, w.nbox, s->err);
       CKL();
       mark(s);
       s->launches++;

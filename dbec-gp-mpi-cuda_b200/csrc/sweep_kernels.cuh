@@ -18,6 +18,8 @@
 // rounding.
 #pragma once
 
+#include <type_traits>
+
 #include "kernels.cuh"
 #include "tma.cuh"
 
@@ -254,7 +256,7 @@ template <int S> __device__ __forceinline__ void wait_stage_free() {
 template <class R, bool CPLX, int AXIS, bool NU, int MSEG, int S, int TWC>
 __global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) k_sweep_xy(const __grid_constant__ CUtensorMap tm_psi,
                                                      const __grid_constant__ CUtensorMap tm_phi, Dims d, SegTab tb,
-                                                     Trap trap, double g, double gd, double dt,
+                                                     Trap trap, LinPhase lin, double g, double gd, double dt,
                                                      const State *__restrict__ st, int tw_arg, int boxn, int nbox,
                                                      uint32_t *err) {
    using P = typename Tr<R, CPLX>::P;
@@ -313,7 +315,25 @@ __global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) k_sweep_xy(const 
       // a timed-out copy makes the whole CTA leave together
       if (__syncthreads_or(!mbar_wait(&full[q], (i / S) & 1, err))) break;
       P *tile = (P *) (base + q * stage_bytes);
-      if (NU) {
+      if constexpr (NU && std::is_same<R, double>::value && !CPLX && AXIS == 0) {
+         // FP64 imaginary time: trap factor exp(-dt V) from the axis tables,
+         // series for the nonlinear part (measured faster than exp of the sum;
+         // in real time CUDA's sincos of the sum measured faster than the
+         // split, so real time keeps nu_op)
+         const int other = t / nzb, z0 = (t - other * nzb) * TW;
+         const R *ptile = (const R *) (tile + rows * TW);
+         const int k = z0 + c;
+         if (k < d.nz) {
+            const int step = blockDim.x >> lg;
+            const double eyz = __ldg((const double *) lin.ey + other) * __ldg((const double *) lin.ez + k);
+            for (int ii = threadIdx.x >> lg; ii < n; ii += step) {
+               const int e = (ii << lg) + c;
+               const double lx = __ldg((const double *) lin.ex + ii) * eyz;
+               tile[e] = nu_split(scl(tile[e], scale), (double) ptile[e], lx, g, gd, dt, (double) invN);
+            }
+         }
+         __syncthreads();
+      } else if constexpr (NU) {
          // every thread keeps one column (blockDim.x is a multiple of TW)
          const int other = t / nzb, z0 = (t - other * nzb) * TW;
          const R *ptile = (const R *) (tile + rows * TW);
