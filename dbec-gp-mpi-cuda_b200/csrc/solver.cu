@@ -414,7 +414,10 @@ static gpe_status plan_tiles(gpe_solver *s) {
       }
       // as many resident CTAs as allowed, then the deepest pipeline (2 or 3
       // stages) that keeps them
-      const int s_hi = s->tune.sweep_stages[ax] > 0 ? s->tune.sweep_stages[ax] : 3;
+      // default depth: 3 for the TMA tensor tiles of the x / y sweeps, 2 for
+      // the z sweep's bulk-copied rows (measured faster on B200 at 256^3, both
+      // modes)
+      const int s_hi = s->tune.sweep_stages[ax] > 0 ? s->tune.sweep_stages[ax] : (ax == 2 ? 2 : 3);
       const int s_lo = s->tune.sweep_stages[ax] > 0 ? s->tune.sweep_stages[ax] : 2;
       if (s_lo < 2 || s_hi > 3) return fail(GPE_ERR_PARAM, "tuning: sweep_stages must be 2 or 3");
       w.ctas = 0;
