@@ -677,7 +677,7 @@ template <class R, bool CPLX> struct Impl {
       return f(std::integral_constant<int, 32>());
    }
    // points per thread of the z passes: (nz/2) L over 256 threads
-   static int zppt(const gpe_solver *s) { return (int) (((s->d.nz / 2) * FftL<R>::L + 255) / 256); }
+   static int zppt(const gpe_solver *s, int L) { return (int) (((s->d.nz / 2) * L + 255) / 256); }
 
    template <bool INV, int L> static gpe_status yfft(gpe_solver *s) {
       const Dims &d = s->d;
@@ -703,35 +703,70 @@ template <class R, bool CPLX> struct Impl {
       return GPE_OK;
    }
 
-   static gpe_status psidd2(gpe_solver *s) {
+   // z pass kernels for a tile of L rows
+   template <int L> static gpe_status zfwd_L(gpe_solver *s, size_t sm) {
       const Dims &d = s->d;
-      constexpr int L = FftL<R>::L;
-      const int h = d.nz / 2;
-      C *spec = (C *) s->spec;
-      const unsigned grows = blocks_for(d.nxy, L);
-      CKS(with_ppt(zppt(s), [&](auto pc) {
+      return with_ppt(zppt(s, L), [&](auto pc) {
          constexpr int PPT = decltype(pc)::value;
-         const size_t sm = 128 + (size_t) L * s->LSr * sizeof(P) + (size_t) h * L * sizeof(C) + d.nz * sizeof(C);
-         CKS(smem_attr((const void *) k_zfwd<R, CPLX, PPT>, sm));
-         k_zfwd<R, CPLX, PPT><<<grows, 256, sm, s->st>>>((const P *) s->psi, spec, d, s->ph, (const C *) s->twz, s->LSr,
-                                                         s->err);
+         CKS(smem_attr((const void *) k_zfwd<R, CPLX, PPT, L>, sm));
+         k_zfwd<R, CPLX, PPT, L><<<blocks_for(d.nxy, L), 256, sm, s->st>>>((const P *) s->psi, (C *) s->spec, d, s->ph,
+                                                                             (const C *) s->twz, s->LSr, s->err);
          CKL();
          mark(s);
          return GPE_OK;
-      }));
+      });
+   }
+
+   template <int L> static gpe_status zinv_L(gpe_solver *s, size_t sm) {
+      const Dims &d = s->d;
+      return with_ppt(zppt(s, L), [&](auto pc) {
+         constexpr int PPT = decltype(pc)::value;
+         CKS(smem_attr((const void *) k_zinv<R, PPT, L>, sm));
+         k_zinv<R, PPT, L><<<blocks_for(d.nxy, L), 256, sm, s->st>>>((const C *) s->spec, (R *) s->phi, d, s->ph,
+                                                                     (const C *) s->twz, s->LSo, s->err);
+         CKL();
+         mark(s);
+         return GPE_OK;
+      });
+   }
+
+   // shared memory of the z passes for L rows; the rows per CTA start at the
+   // preferred value and halve (down to 4) until the tile fits
+   static size_t zfwd_smem(const gpe_solver *s, int L) {
+      const Dims &d = s->d;
+      return 128 + (size_t) L * s->LSr * sizeof(P) + (size_t) (d.nz / 2) * L * sizeof(C) + d.nz * sizeof(C);
+   }
+   static size_t zinv_smem(const gpe_solver *s, int L) {
+      const Dims &d = s->d;
+      const size_t in_el = std::max((size_t) L * d.nzp, ((size_t) L * s->LSo * sizeof(R) + sizeof(C) - 1) / sizeof(C));
+      return 128 + ((in_el + 7) & ~(size_t) 7) * sizeof(C) + (size_t) (d.nz / 2) * L * sizeof(C) + d.nz * sizeof(C);
+   }
+   template <class SM> static int zrows(const gpe_solver *s, int pref, SM smem) {
+      int L = pref;
+      while (L > 4 && smem(s, L) > 227 * 1024) L /= 2;
+      return L;
+   }
+   template <class F> static gpe_status with_zrows(int L, F f) {
+      if (L == 16) return f(std::integral_constant<int, 16>());
+      if (L == 8) return f(std::integral_constant<int, 8>());
+      return f(std::integral_constant<int, 4>());
+   }
+
+   static gpe_status psidd2(gpe_solver *s) {
+      const Dims &d = s->d;
+      {
+         const int L = zrows(s, ZRows<R, CPLX>::fwd, zfwd_smem);
+         const size_t sm = zfwd_smem(s, L);
+         CKS(with_zrows(L, [&](auto lc) { return zfwd_L<decltype(lc)::value>(s, sm); }));
+      }
       CKS(with_L(s->Ly, [&](auto Lc) { return yfft<false, decltype(Lc)::value>(s); }));
       CKS(with_L(s->Lx, [&](auto Lc) { return xconv<decltype(Lc)::value>(s); }));
       CKS(with_L(s->Ly, [&](auto Lc) { return yfft<true, decltype(Lc)::value>(s); }));
-      CKS(with_ppt(zppt(s), [&](auto pc) {
-         constexpr int PPT = decltype(pc)::value;
-         const size_t in_el = std::max((size_t) L * d.nzp, ((size_t) L * s->LSo * sizeof(R) + sizeof(C) - 1) / sizeof(C));
-         const size_t sm = 128 + ((in_el + 7) & ~(size_t) 7) * sizeof(C) + (size_t) h * L * sizeof(C) + d.nz * sizeof(C);
-         CKS(smem_attr((const void *) k_zinv<R, PPT>, sm));
-         k_zinv<R, PPT><<<grows, 256, sm, s->st>>>(spec, (R *) s->phi, d, s->ph, (const C *) s->twz, s->LSo, s->err);
-         CKL();
-         mark(s);
-         return GPE_OK;
-      }));
+      {
+         const int L = zrows(s, ZRows<R, CPLX>::inv, zinv_smem);
+         const size_t sm = zinv_smem(s, L);
+         CKS(with_zrows(L, [&](auto lc) { return zinv_L<decltype(lc)::value>(s, sm); }));
+      }
       k_phifix<R><<<256, 256, 0, s->st>>>((R *) s->phi, d);
       CKL();
       mark(s);

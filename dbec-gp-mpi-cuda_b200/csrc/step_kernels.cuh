@@ -29,6 +29,15 @@ template <class R> struct FftL {
    static constexpr int PPT = sizeof(R) == 8 ? 8 : 16;
 };
 
+// Preferred rows per CTA of the z passes: 16, so that their radix-8 stages
+// (nz/2-point lines) keep all 256 threads busy, except the forward pass over
+// complex FP64 rows (4 KB each), which measured faster with 8 rows and four
+// CTAs per SM.  The host halves it while the tile does not fit shared memory.
+template <class R, bool CPLX> struct ZRows {
+   static constexpr int fwd = (sizeof(R) == 8 && CPLX) ? 8 : 16;
+   static constexpr int inv = 16;
+};
+
 // |psi|^2 of L rows (row stride LS elements) packed as complex lines of
 // length h = nz/2 in the interleaved layout: buf[m L + l] = (rho[2m], rho[2m+1]).
 template <class R, bool CPLX, int L>
@@ -63,13 +72,13 @@ __device__ __forceinline__ void zfwd_split(const cpx<R> *Z, const cpx<R> *tw, in
 }
 
 // Pass 1: |psi|^2 rows -> half spectrum rows (L rows per CTA).
-template <class R, bool CPLX, int PPT>
+template <class R, bool CPLX, int PPT, int L>
 __global__ void __launch_bounds__(256, 4) k_zfwd(const typename Tr<R, CPLX>::P *__restrict__ psi,
                                               cpx<R> *__restrict__ spec, Dims d, FftPlan ph,
                                               const cpx<R> *__restrict__ twz, int LSr, uint32_t *err) {
    using C = cpx<R>;
    using P = typename Tr<R, CPLX>::P;
-   constexpr int L = FftL<R>::L;
+
    extern __shared__ __align__(16) unsigned char smem_raw[];
    __shared__ __align__(8) uint64_t bar;
    const int nz = d.nz, h = nz / 2, nzh = d.nzh, nzp = d.nzp;
@@ -192,11 +201,11 @@ __global__ void __launch_bounds__(256, 4) k_xconv(const __grid_constant__ CUtens
 }
 
 // Pass 5: half spectrum rows -> phi rows (unnormalised inverse, Hermitian).
-template <class R, int PPT>
+template <class R, int PPT, int L>
 __global__ void __launch_bounds__(256, 4) k_zinv(const cpx<R> *__restrict__ spec, R *__restrict__ phi, Dims d,
                                                  FftPlan ph, const cpx<R> *__restrict__ twz, int LSo, uint32_t *err) {
    using C = cpx<R>;
-   constexpr int L = FftL<R>::L;
+
    extern __shared__ __align__(16) unsigned char smem_raw[];
    __shared__ __align__(8) uint64_t bar;
    const int nz = d.nz, h = nz / 2, nzp = d.nzp;
