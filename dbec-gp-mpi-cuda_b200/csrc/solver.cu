@@ -1362,8 +1362,7 @@ extern "C" double gpe_step_kernel_bytes(gpe_solver *s, int i) {
    const double sp = (double) s->esz_psi, sc = (double) s->esz_c, r = (double) s->esz_r;
    const double npts = (double) d.npts, half = (double) d.nzh * (double) d.nxy;
    const double oct = (double) d.nzh * (d.nx / 2 + 1) * (d.ny / 2 + 1) * 8.;
-   const double planes = ((double) (d.ny - 1) * (d.nz - 1) + (double) (d.nx - 1) * (d.nz - 1) +
-                          (double) (d.nx - 1) * (d.ny - 1)) * 2. * r;
+   const double planes = ((double) (d.ny - 1) * (d.nz - 1) + (double) (d.nx - 1) * (d.nz - 1)) * 2. * r;
    switch (i) {
    case 0: return npts * sp + half * sc;
    case 1: case 3: return 2. * half * sc;

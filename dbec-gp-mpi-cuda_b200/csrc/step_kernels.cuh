@@ -248,6 +248,14 @@ __global__ void __launch_bounds__(256, 4) k_zinv(const cpx<R> *__restrict__ spec
       out[l * LSo + 2 * m] = v.x;
       out[l * LSo + 2 * m + 1] = v.y;
    }
+   __syncthreads();
+   // boundary plane z = nz-1 <- z = 0 for x < nx-1, y < ny-1, inside the row
+   // (the z part of calcpsidd2_kernel2b, imag3d-mpicuda.cu:1605-1625)
+   if (threadIdx.x < nr) {
+      const long long row = r0 + threadIdx.x;
+      const long long x = row / d.ny, y = row - x * d.ny;
+      if (x < d.nx - 1 && y < d.ny - 1) out[threadIdx.x * LSo + nz - 1] = out[threadIdx.x * LSo];
+   }
    fence_proxy_async();
    __syncthreads();
    if (threadIdx.x == 0) {
@@ -258,25 +266,22 @@ __global__ void __launch_bounds__(256, 4) k_zinv(const cpx<R> *__restrict__ spec
 }
 
 // Boundary planes of phi at one rank (calcpsidd2_kernel2a/2b with last = 1,
-// imag3d-mpicuda.cu:1591-1625): x = nx-1 <- x = 0, y = ny-1 <- y = 0,
-// z = nz-1 <- z = 0, each excluding the other two last indices.  The read
-// and write sets are disjoint, so all three copies run concurrently.
+// imag3d-mpicuda.cu:1591-1625): x = nx-1 <- x = 0 and y = ny-1 <- y = 0 here,
+// each excluding the other two last indices; z = nz-1 <- z = 0 is done inside
+// the rows by k_zinv.  The read and write sets are disjoint, so both copies
+// run concurrently.
 template <class R>
 __global__ void k_phifix(R *__restrict__ phi, Dims d) {
    const long long A = (long long) (d.ny - 1) * (d.nz - 1);
    const long long B = (long long) (d.nx - 1) * (d.nz - 1);
-   const long long Cn = (long long) (d.nx - 1) * (d.ny - 1);
-   const long long tot = A + B + Cn;
-   for (long long e = blockIdx.x * (long long) blockDim.x + threadIdx.x; e < tot; e += (long long) gridDim.x * blockDim.x) {
+   for (long long e = blockIdx.x * (long long) blockDim.x + threadIdx.x; e < A + B;
+        e += (long long) gridDim.x * blockDim.x) {
       if (e < A) {
          const long long j = e / (d.nz - 1), k = e - j * (d.nz - 1);
          phi[((long long) (d.nx - 1) * d.ny + j) * d.nz + k] = phi[j * d.nz + k];
-      } else if (e < A + B) {
+      } else {
          const long long q = e - A, i = q / (d.nz - 1), k = q - i * (d.nz - 1);
          phi[(i * d.ny + d.ny - 1) * d.nz + k] = phi[(i * d.ny) * d.nz + k];
-      } else {
-         const long long q = e - A - B, i = q / (d.ny - 1), j = q - i * (d.ny - 1);
-         phi[(i * d.ny + j) * d.nz + d.nz - 1] = phi[(i * d.ny + j) * d.nz];
       }
    }
 }
