@@ -72,8 +72,10 @@ __device__ __forceinline__ void zfwd_split(const cpx<R> *Z, const cpx<R> *tw, in
 }
 
 // Pass 1: |psi|^2 rows -> half spectrum rows (L rows per CTA).
+// Register budget: four CTAs per SM for 8-row tiles, three for 16-row tiles
+// (whose shared tiles allow no more; measured faster with the larger budget).
 template <class R, bool CPLX, int PPT, int L>
-__global__ void __launch_bounds__(256, 4) k_zfwd(const typename Tr<R, CPLX>::P *__restrict__ psi,
+__global__ void __launch_bounds__(256, L >= 16 ? 3 : 4) k_zfwd(const typename Tr<R, CPLX>::P *__restrict__ psi,
                                               cpx<R> *__restrict__ spec, Dims d, FftPlan ph,
                                               const cpx<R> *__restrict__ twz, int LSr, uint32_t *err) {
    using C = cpx<R>;
@@ -202,7 +204,7 @@ __global__ void __launch_bounds__(256, 4) k_xconv(const __grid_constant__ CUtens
 
 // Pass 5: half spectrum rows -> phi rows (unnormalised inverse, Hermitian).
 template <class R, int PPT, int L>
-__global__ void __launch_bounds__(256, 4) k_zinv(const cpx<R> *__restrict__ spec, R *__restrict__ phi, Dims d,
+__global__ void __launch_bounds__(256, L >= 16 ? 3 : 4) k_zinv(const cpx<R> *__restrict__ spec, R *__restrict__ phi, Dims d,
                                                  FftPlan ph, const cpx<R> *__restrict__ twz, int LSo, uint32_t *err) {
    using C = cpx<R>;
 
