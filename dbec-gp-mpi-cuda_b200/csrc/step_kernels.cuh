@@ -78,6 +78,8 @@ template <class R, bool CPLX, int PPT, int L>
 __global__ void __launch_bounds__(256, L >= 16 ? 3 : 4) k_zfwd(const typename Tr<R, CPLX>::P *__restrict__ psi,
                                               cpx<R> *__restrict__ spec, Dims d, FftPlan ph,
                                               const cpx<R> *__restrict__ twz, int LSr, uint32_t *err) {
+   pdl_trigger();
+   pdl_wait();
    using C = cpx<R>;
    using P = typename Tr<R, CPLX>::P;
 
@@ -122,6 +124,8 @@ __global__ void __launch_bounds__(256, L >= 16 ? 3 : 4) k_zfwd(const typename Tr
 template <class R, bool INV, int L>
 __global__ void __launch_bounds__(256, 4) k_yfft(const __grid_constant__ CUtensorMap tm, Dims d, FftPlan py,
                                                  const cpx<R> *__restrict__ twy, int boxn, int nbox, uint32_t *err) {
+   pdl_trigger();
+   pdl_wait();
    using C = cpx<R>;
    constexpr int PPT = FftL<R>::PPT;
    extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -159,6 +163,8 @@ template <class R, int L>
 __global__ void __launch_bounds__(256, 4) k_xconv(const __grid_constant__ CUtensorMap tm, Dims d, FftPlan px,
                                                   const cpx<R> *__restrict__ twx, const double *__restrict__ udd,
                                                   const State *__restrict__ st, int boxn, int nbox, uint32_t *err) {
+   pdl_trigger();
+   pdl_wait();
    using C = cpx<R>;
    constexpr int PPT = FftL<R>::PPT;
    extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -206,6 +212,8 @@ __global__ void __launch_bounds__(256, 4) k_xconv(const __grid_constant__ CUtens
 template <class R, int PPT, int L>
 __global__ void __launch_bounds__(256, L >= 16 ? 3 : 4) k_zinv(const cpx<R> *__restrict__ spec, R *__restrict__ phi, Dims d,
                                                  FftPlan ph, const cpx<R> *__restrict__ twz, int LSo, uint32_t *err) {
+   pdl_trigger();
+   pdl_wait();
    using C = cpx<R>;
 
    extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -274,6 +282,8 @@ __global__ void __launch_bounds__(256, L >= 16 ? 3 : 4) k_zinv(const cpx<R> *__r
 // run concurrently.
 template <class R>
 __global__ void k_phifix(R *__restrict__ phi, Dims d) {
+   pdl_trigger();
+   pdl_wait();
    const long long A = (long long) (d.ny - 1) * (d.nz - 1);
    const long long B = (long long) (d.nx - 1) * (d.nz - 1);
    for (long long e = blockIdx.x * (long long) blockDim.x + threadIdx.x; e < A + B;
@@ -350,6 +360,8 @@ constexpr int kNormRowsPerCta = 8;
 __global__ void __launch_bounds__(32 * kNormRowsPerCta) k_norm_final(const double *__restrict__ rowsum, Dims d,
                                                                      double hx, double hy, State *st, double *xs,
                                                                      double *out_norm) {
+   pdl_trigger();
+   pdl_wait();
    const int lane = threadIdx.x & 31;
    const int i = blockIdx.x * kNormRowsPerCta + (threadIdx.x >> 5);
    if (i < d.nx) {
@@ -409,6 +421,8 @@ __global__ void __launch_bounds__(32 * kNormRowsPerCta) k_rms_final(const double
                                                                     double hy, const double *__restrict__ x2,
                                                                     const double *__restrict__ y2, State *st,
                                                                     double *xs, double *__restrict__ out) {
+   pdl_trigger();
+   pdl_wait();
    const int lane = threadIdx.x & 31;
    const int i = blockIdx.x * kNormRowsPerCta + (threadIdx.x >> 5);
    if (i < d.nx) {

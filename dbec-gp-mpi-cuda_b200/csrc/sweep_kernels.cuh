@@ -259,6 +259,8 @@ __global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) k_sweep_xy(const 
                                                      Trap trap, LinPhase lin, double g, double gd, double dt,
                                                      const State *__restrict__ st, int tw_arg, int boxn, int nbox,
                                                      uint32_t *err) {
+   pdl_trigger();
+   pdl_wait();
    using P = typename Tr<R, CPLX>::P;
    const int TW = TWC > 0 ? TWC : tw_arg;
    extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -375,6 +377,8 @@ __global__ void __launch_bounds__(256, kSweepCtas[0]) k_sweep_z(typename Tr<R, C
                                                     const double *__restrict__ wz2, double hz3,
                                                     double *__restrict__ rowsum, double *__restrict__ rowsum2,
                                                     uint32_t *err) {
+   pdl_trigger();
+   pdl_wait();
    constexpr bool SIMP = MOM >= 1;
    const int TR = TWC > 0 ? TWC : tr_arg;
    using P = typename Tr<R, CPLX>::P;

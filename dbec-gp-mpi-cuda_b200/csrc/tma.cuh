@@ -17,6 +17,15 @@ enum : uint32_t { kErrTmaTimeout = 1u };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t) __cvta_generic_to_shared(p); }
 
+// Programmatic dependent launch.  pdl_trigger lets the next kernel of the
+// stream be scheduled once every CTA of this grid has started; pdl_wait
+// returns once the previous kernel has completed and its memory is visible.
+// Every step kernel calls both before its first global-memory access, so a
+// kernel launched with the attribute can occupy SMs freed by the tail of its
+// predecessor without reading or writing anything early.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
