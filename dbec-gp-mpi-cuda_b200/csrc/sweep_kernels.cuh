@@ -93,7 +93,11 @@ template <class R, bool CPLX> struct SegOps {
 // shared scratch of 2 * (NW + 1) * TW elements (NW warps hold segments).
 // Writes the swept line back in place.  When simp_w is non-null, *simp
 // receives this thread's share of sum_i simp_w[i] |psi'_i|^2, and when
-// simp_w2 is non-null *simp2 that of sum_i simp_w2[i] |psi'_i|^2.
+// simp_w2 is non-null *simp2 that of sum_i simp_w2[i] |psi'_i|^2.  Every
+// value of the line the recurrence reads goes through xf(value, i) first
+// (the fused calcnu of the x sweep; identity otherwise); a thread reads its
+// own points and the two above its segment, so no transformed copy of the
+// line is stored.
 //
 // Carries: segment p maps the value entering at its top (index hf+1) to the
 // value at its bottom (index lo) by the affine map x -> b + a x with
@@ -101,11 +105,15 @@ template <class R, bool CPLX> struct SegOps {
 // of the maps of all segments above it: a suffix scan, done with shuffles
 // inside a warp and a short chain over the warps above.  The forward
 // recurrence composes x -> psi'~[hf+1] + N[hf+1] x from the bottom (prefix).
-template <class R, bool CPLX, int MSEG, int TWC = 0>
+struct NoXf {
+   template <class P> __device__ __forceinline__ P operator()(P v, int) const { return v; }
+};
+
+template <class R, bool CPLX, int MSEG, int TWC = 0, class XF = NoXf>
 __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, int cs, int c, int p, int tw_arg,
                                           const SegTab &tb, typename Tr<R, CPLX>::P *blk, const double *simp_w,
                                           double *simp, const double *simp_w2 = nullptr,
-                                          double *simp2 = nullptr) {
+                                          double *simp2 = nullptr, const XF &xf = XF()) {
    using Op = SegOps<R, CPLX>;
    using P = typename Tr<R, CPLX>::P;
    const int TW = TWC > 0 ? TWC : tw_arg;  // lines per CTA (compile time when TWC > 0)
@@ -120,7 +128,7 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
    const int K = hf - lo + 1;                // owned points, 1 <= K <= MSEG
    const R a = CPLX ? (R) tb.A.y : (R) tb.A.x;
    P *line = s + c * cs;
-   auto L = [&](int i) -> P { return line[i * es]; };
+   auto L = [&](int i) -> P { return xf(line[i * es], i); };
    P *ba = blk, *bb = blk + (NW + 1) * TW;  // per-warp block maps [NW][TW]
    const unsigned fullmask = 0xffffffffu;
 
@@ -230,6 +238,23 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
    if (simp2) *simp2 = acc2;
 }
 
+// calcnu fused into the x sweep's reads (calcnu_kernel imag3d-mpicuda.cu:1759,
+// real3d-mpicuda.cu:1856): element i of column c of the tile, with the
+// pending 1/norm applied first; V is recomputed from the trap tables (the
+// terms of the two fixed coordinates hoisted per column).
+template <class R> struct NuTrap {
+   const R *ptile;  // phi tile, row stride tw
+   int tw;
+   const double *va;
+   double ca, to, tz, hp, scale;
+   R g, gd, dt, invN;
+   template <class P> __device__ __forceinline__ P operator()(P v, int i) const {
+      const double sv = arn(arn(mrn(ca, va[i]), to), tz);
+      const R V = (R) mrn(hp, sv);
+      return nu_op<R>(scl(v, scale), ptile[i * tw], V, g, gd, dt, invN);
+   }
+};
+
 // ---------------------------------------------------------------------------
 // Persistent pipelined CTAs.  A CTA walks the tiles t = blockIdx.x,
 // blockIdx.x + gridDim.x, ... through S shared-memory stages: while it sweeps
@@ -335,7 +360,7 @@ __global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) k_sweep_xy(const 
             }
          }
          __syncthreads();
-      } else if constexpr (NU) {
+      } else if constexpr (NU && std::is_same<R, double>::value) {
          // every thread keeps one column (blockDim.x is a multiple of TW)
          const int other = t / nzb, z0 = (t - other * nzb) * TW;
          const R *ptile = (const R *) (tile + rows * TW);
@@ -357,7 +382,20 @@ __global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) k_sweep_xy(const 
          }
          __syncthreads();
       }
-      seg_sweep<R, CPLX, MSEG, TWC>(tile, TW, 1, c, p, TW, tb, blk, nullptr, nullptr);
+      if constexpr (NU && std::is_same<R, float>::value) {
+         // FP32: calcnu on the sweep's reads (measured faster than the
+         // separate pass over the tile; slower in FP64, where a thread's
+         // extra evaluations for the two points above its segment cost more)
+         const int other = t / nzb, z0 = (t - other * nzb) * TW;
+         const int k = min(z0 + c, d.nz - 1);  // columns past nz are zero fill, never stored
+         const double tz = mrn(trap.vl2, trap.z2[k]);
+         const double to = AXIS == 0 ? mrn(trap.vn2, trap.y2[other]) : mrn(trap.vg2, trap.x2[other]);
+         const NuTrap<R> xf{(const R *) (tile + rows * TW) + c, TW, AXIS == 0 ? trap.x2 : trap.y2,
+                            AXIS == 0 ? trap.vg2 : trap.vn2, to, tz, trap.hp, scale, (R) g, (R) gd, (R) dt, invN};
+         seg_sweep<R, CPLX, MSEG, TWC>(tile, TW, 1, c, p, TW, tb, blk, nullptr, nullptr, nullptr, nullptr, xf);
+      } else {
+         seg_sweep<R, CPLX, MSEG, TWC>(tile, TW, 1, c, p, TW, tb, blk, nullptr, nullptr);
+      }
       fence_proxy_async();
       __syncthreads();
       if (threadIdx.x == 0) copy_tile(t, q, false);
