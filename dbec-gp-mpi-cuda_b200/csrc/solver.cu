@@ -428,17 +428,21 @@ static gpe_status plan_tiles(gpe_solver *s) {
       w.smem = fixed + w.S * stage;
    }
    // spectrum tiles: spec[x][y][kz] viewed as [nx][ny][2 nzh] scalars; L kz
-   // columns (128-byte rows) per tile, halved (down to 2) until a tile of a
-   // whole line holds at most 256 PPT points (32 KB), the in-place FFT's
-   // register budget
+   // columns (at most a 128-byte row) per tile, halved (down to 2) until a
+   // tile of a whole line holds at most 256 PPT points (32 KB), the in-place
+   // FFT's register budget; the CTA has one thread per PPT points of its tile
    {
       s->boxy = (int) std::min<long>(d.ny, 256);
       s->nboxy = (d.ny + s->boxy - 1) / s->boxy;
       s->boxx = (int) std::min<long>(d.nx, 256);
       s->nboxx = (d.nx + s->boxx - 1) / s->boxx;
       const long ppt = s->fp32 ? 16 : 8;  // FftL<R>::PPT
+      // FP64 starts from 4 columns: on B200 the 128-thread CTAs of 4-column
+      // tiles (eight per SM) measured faster than 8-column tiles (four per
+      // SM): y pass 60 -> 56 us, 256^3 step 0.870 -> 0.863 ms; FP32 widths
+      // measured alike
       auto pickL = [&](long rows) {
-         int L = 128 / (int) s->esz_c;
+         int L = s->fp32 ? 128 / (int) s->esz_c : 4;
          while (L > 2 && rows * L > 256 * ppt) L /= 2;
          return L;
       };
@@ -701,12 +705,19 @@ template <class R, bool CPLX> struct Impl {
    // points per thread of the z passes: (nz/2) L over 256 threads
    static int zppt(const gpe_solver *s, int L) { return (int) (((s->d.nz / 2) * L + 255) / 256); }
 
+   // threads of a y / x pass CTA: PPT points each over a tile of rows x L
+   // (at most 256: the kernels' register budget)
+   static unsigned fft_threads(long rows, int L) {
+      const long t = (rows * L + FftL<R>::PPT - 1) / FftL<R>::PPT;
+      return (unsigned) std::min<long>(256, std::max<long>(32, (t + 31) / 32 * 32));
+   }
+
    template <bool INV, int L> static gpe_status yfft(gpe_solver *s) {
       const Dims &d = s->d;
       const int nkb = (d.nzh + L - 1) / L;
       const size_t smy = 128 + (size_t) s->boxy * s->nboxy * L * sizeof(C) + d.ny * sizeof(C);
       CKS(smem_attr((const void *) k_yfft<R, INV, L>, smy));
-      CKS(launch_pdl(k_yfft<R, INV, L>, (unsigned) (d.nx * nkb), 256, smy, s, s->tm_spec_y, d, s->py,
+      CKS(launch_pdl(k_yfft<R, INV, L>, (unsigned) (d.nx * nkb), fft_threads(s->boxy * s->nboxy, L), smy, s, s->tm_spec_y, d, s->py,
                      (const C *) s->twy, s->boxy, s->nboxy, s->err));
       CKL();
       mark(s);
@@ -718,7 +729,7 @@ template <class R, bool CPLX> struct Impl {
       const int nkb = (d.nzh + L - 1) / L;
       const size_t sm = 128 + (size_t) s->boxx * s->nboxx * L * sizeof(C) + d.nx * sizeof(C);
       CKS(smem_attr((const void *) k_xconv<R, L>, sm));
-      CKS(launch_pdl(k_xconv<R, L>, (unsigned) (d.ny * nkb), 256, sm, s, s->tm_spec_x, d, s->px, (const C *) s->twx, s->udd,
+      CKS(launch_pdl(k_xconv<R, L>, (unsigned) (d.ny * nkb), fft_threads(s->boxx * s->nboxx, L), sm, s, s->tm_spec_x, d, s->px, (const C *) s->twx, s->udd,
                                                                  s->state, s->boxx, s->nboxx, s->err));
       CKL();
       mark(s);

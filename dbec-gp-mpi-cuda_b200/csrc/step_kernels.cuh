@@ -119,8 +119,10 @@ __global__ void __launch_bounds__(256, L >= 16 ? 3 : 4) k_zfwd(const typename Tr
    }
 }
 
-// Passes 2 and 4: FFT along y of L kz columns of one x plane (L chosen by the
-// host so that three CTAs fit on an SM).
+// Passes 2 and 4: FFT along y of L kz columns of one x plane.  The host sizes
+// the CTA at one thread per PPT points of the tile (128 threads for the
+// 4-column FP64 tiles, so that eight fit on an SM); the register budget
+// (launch bounds 256 x 4) allows any of these sizes.
 template <class R, bool INV, int L>
 __global__ void __launch_bounds__(256, 4) k_yfft(const __grid_constant__ CUtensorMap tm, Dims d, FftPlan py,
                                                  const cpx<R> *__restrict__ twy, int boxn, int nbox, uint32_t *err) {
@@ -157,8 +159,8 @@ __global__ void __launch_bounds__(256, 4) k_yfft(const __grid_constant__ CUtenso
 }
 
 // Pass 3: FFT along x, multiply by Udd(k) * scale^2, inverse FFT along x, for
-// L kz columns of one y plane.  Udd octant layout [|kx|][|ky|][kz].  Compiled
-// for three resident CTAs per SM (the host picks L so that their tiles fit).
+// L kz columns of one y plane.  Udd octant layout [|kx|][|ky|][kz].  CTA size
+// as for the y passes.
 template <class R, int L>
 __global__ void __launch_bounds__(256, 4) k_xconv(const __grid_constant__ CUtensorMap tm, Dims d, FftPlan px,
                                                   const cpx<R> *__restrict__ twx, const double *__restrict__ udd,
