@@ -420,8 +420,12 @@ static gpe_status plan_tiles(gpe_solver *s) {
       const int s_hi = s->tune.sweep_stages[ax] > 0 ? s->tune.sweep_stages[ax] : (ax == 2 ? 2 : 3);
       const int s_lo = s->tune.sweep_stages[ax] > 0 ? s->tune.sweep_stages[ax] : 2;
       if (s_lo < 2 || s_hi > 3) return fail(GPE_ERR_PARAM, "tuning: sweep_stages must be 2 or 3");
+      // the register budget of max_ctas CTAs of 256 threads holds more CTAs
+      // of fewer threads
+      const int thr = (w.TW * P + 31) & ~31;
+      const int ct_max = std::min(32, 256 * max_ctas / thr);
       w.ctas = 0;
-      for (int ct = max_ctas; ct >= 1 && !w.ctas; ct--)
+      for (int ct = ct_max; ct >= 1 && !w.ctas; ct--)
          for (int S = s_hi; S >= s_lo && !w.ctas; S--)
             if ((fixed + S * stage) * ct <= sm_cap) { w.ctas = ct; w.S = S; }
       if (!w.ctas) return fail(GPE_ERR_PARAM, "grid too large for the sweep tiles (shared memory)");
