@@ -738,7 +738,8 @@ template <class R, bool CPLX> struct Impl {
    template <int L> static gpe_status xconv(gpe_solver *s) {
       const Dims &d = s->d;
       const int nkb = (d.nzh + L - 1) / L;
-      const size_t sm = 128 + (size_t) s->boxx * s->nboxx * L * sizeof(C) + d.nx * sizeof(C);
+      const size_t sm = 128 + (size_t) s->boxx * s->nboxx * L * sizeof(C) + d.nx * sizeof(C) +
+                        (size_t) (d.nx / 2 + 1) * L * sizeof(double);
       CKS(smem_attr((const void *) k_xconv<R, L>, sm));
       CKS(launch_pdl(k_xconv<R, L>, (unsigned) (d.ny * nkb), fft_threads(s->boxx * s->nboxx, L), sm, s, s->tm_spec_x, d, s->px, (const C *) s->twx, s->udd,
                                                                  s->state, s->boxx, s->nboxx, s->err));

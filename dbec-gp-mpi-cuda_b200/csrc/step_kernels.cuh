@@ -177,8 +177,11 @@ __global__ void __launch_bounds__(256, 4) k_xconv(const __grid_constant__ CUtens
    const int nx = d.nx, ny = d.ny, rows = boxn * nbox;
    C *buf = (C *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
    C *tw = buf + rows * L;
+   double *ud = (double *) (tw + nx);  // Udd of this y plane and these columns, [|kx|][L]
    const int nkb = (d.nzh + L - 1) / L;
    const int y = blockIdx.x / nkb, k0 = (blockIdx.x - y * nkb) * L;
+   const int nxh = nx / 2 + 1, nyh = ny / 2 + 1, nzh = d.nzh;
+   const int ay = (y <= ny / 2) ? y : ny - y;
    if (threadIdx.x == 0) {
       mbar_init(&bar, 1);
       fence_mbar_init();
@@ -189,17 +192,26 @@ __global__ void __launch_bounds__(256, 4) k_xconv(const __grid_constant__ CUtens
       bulk_load(tw, twx, (uint32_t) (nx * sizeof(C)), &bar);
       for (int b = 0; b < nbox; b++) tma_load_3d(buf + b * boxn * L, &tm, 2 * k0, y, b * boxn, &bar);
    }
-   if (__syncthreads_or(!mbar_wait(&bar, 0, err))) return;
+   // the Udd factors of the tile travel while the tile and the forward FFT do
+   // (loaded after the FFT, their latency measured exposed)
+   for (int e = threadIdx.x; e < nxh * L; e += blockDim.x) {
+      const int ax = e / L, c = e - ax * L;
+      const int k = k0 + c < nzh ? k0 + c : nzh - 1;
+      cp_async8(ud + e, udd + ((long long) ax * nyh + ay) * nzh + k);
+   }
+   if (__syncthreads_or(!mbar_wait(&bar, 0, err))) {
+      cp_async_wait_all();
+      return;
+   }
    fft_lines_ip<L, C, false, PPT>(buf, px, tw, 1);
+   cp_async_wait_all();
+   __syncthreads();
    C *res = buf;
    const double s2 = st->scale2;
-   const int nyh = ny / 2 + 1, nzh = d.nzh;
-   const int ay = (y <= ny / 2) ? y : ny - y;
    for (int e = threadIdx.x; e < nx * L; e += blockDim.x) {
       const int xx = e / L, c = e - xx * L;
-      const int k = k0 + c < nzh ? k0 + c : nzh - 1;
       const int ax = (xx <= nx / 2) ? xx : nx - xx;
-      const R u = (R) (udd[((long long) ax * nyh + ay) * nzh + k] * s2);
+      const R u = (R) (ud[ax * L + c] * s2);
       res[e] = cscale(res[e], u);
    }
    __syncthreads();

@@ -26,6 +26,14 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t) 
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
+// Asynchronous 8-byte global -> shared copies (cp.async); cp_async_wait_all
+// returns once all of this thread's copies have landed (each thread then
+// still needs a barrier before others read them).
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
