@@ -375,10 +375,13 @@ static gpe_status plan_tiles(gpe_solver *s) {
          if (ax < 2) {
             const long rows = (long) std::min<long>(nn[ax], 256) * ((nn[ax] + 255) / 256);
             stage = (rows * TW * esz + (ax == 0 ? rows * TW * rsz : 0) + 127) & ~(size_t) 127;
-            fixed = 128 + blk + (ax == 0 ? (size_t) nn[0] * sizeof(double) : 0);
+            // FP64 x sweep: calcnu's per-x table staged in shared memory
+            fixed = 128 + blk + (ax == 0 && !s->fp32 ? (size_t) nn[0] * sizeof(double) : 0);
          } else {
             stage = ((size_t) TW * (d.nz + 16 / esz) * esz + 127) & ~(size_t) 127;
-            fixed = 128 + blk + 2 * (size_t) P * TW * sizeof(double);
+            // FP64: the four coefficient tables staged in shared memory
+            fixed = 128 + blk + 2 * (size_t) P * TW * sizeof(double) +
+                    (s->fp32 ? 0 : 4 * (size_t) nn[2] * (s->cplx ? 16 : 8));
          }
       };
       int pick = 0;

@@ -43,6 +43,15 @@ template <class R, bool CPLX> struct SegOps {
          return (R) __ldg((const double *) t + i);
       }
    }
+   // the same from a table staged in shared memory
+   __device__ static P lds(const void *t, int i) {
+      if constexpr (CPLX) {
+         const double2 v = ((const double2 *) t)[i];
+         return mk<R>((R) v.x, (R) v.y);
+      } else {
+         return (R) ((const double *) t)[i];
+      }
+   }
    __device__ static P cv(double2 v) {
       if constexpr (CPLX) return mk<R>((R) v.x, (R) v.y);
       else return (R) v.x;
@@ -109,7 +118,7 @@ struct NoXf {
    template <class P> __device__ __forceinline__ P operator()(P v, int) const { return v; }
 };
 
-template <class R, bool CPLX, int MSEG, int TWC = 0, class XF = NoXf>
+template <class R, bool CPLX, int MSEG, int TWC = 0, class XF = NoXf, bool STAB = false>
 __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, int cs, int c, int p, int tw_arg,
                                           const SegTab &tb, typename Tr<R, CPLX>::P *blk, const double *simp_w,
                                           double *simp, const double *simp_w2 = nullptr,
@@ -129,6 +138,8 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
    const R a = CPLX ? (R) tb.A.y : (R) tb.A.x;
    P *line = s + c * cs;
    auto L = [&](int i) -> P { return xf(line[i * es], i); };
+   // coefficient tables: global (read-only path) or staged in shared memory
+   auto T = [&](const void *t, int i) -> P { return STAB ? Op::lds(t, i) : Op::ld(t, i); };
    P *ba = blk, *bb = blk + (NW + 1) * TW;  // per-warp block maps [NW][TW]
    const unsigned fullmask = 0xffffffffu;
 
@@ -143,7 +154,7 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
       for (int q = MSEG - 1; q >= 0; q--) {
          if (q < K) {
             const P w0 = L(lo + q);
-            b = Op::back_step(b, w2, w1, w0, Op::ld(tb.ga, lo + q + 1), a);
+            b = Op::back_step(b, w2, w1, w0, T(tb.ga, lo + q + 1), a);
             bt[q] = b;
             w2 = w1;
             w1 = w0;
@@ -153,7 +164,7 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
    // ---- suffix scan of the backward maps: in-warp, then over the warps above
    P sa = zero_of<P>(), sb = zero_of<P>();
    if (act) {
-      sa = top ? zero_of<P>() : Op::ld(tb.M, lo);
+      sa = top ? zero_of<P>() : T(tb.M, lo);
       sb = bt[0];
    }
    for (int dd = 1; dd < SPW; dd <<= 1) {
@@ -188,12 +199,12 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
       for (int q = 0; q < MSEG; q++) {
          if (q < K) {
             const int i = lo + q;
-            const P beta = Op::fma_(Op::ld(tb.M, i), bin, bt[q]);
-            v = Op::fma_(Op::ld(tb.al, i), v, beta);
+            const P beta = Op::fma_(T(tb.M, i), bin, bt[q]);
+            v = Op::fma_(T(tb.al, i), v, beta);
             bt[q] = v;
          }
       }
-      sa = Op::ld(tb.N, hf + 1);
+      sa = T(tb.N, hf + 1);
    }
    // ---- prefix scan of the forward maps
    sb = v;
@@ -221,7 +232,7 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
          for (int q = 0; q < MSEG; q++) {
             if (q < K) {
                const int k = lo + q + 1;
-               const P val = Op::fma_(Op::ld(tb.N, k), fin, bt[q]);
+               const P val = Op::fma_(T(tb.N, k), fin, bt[q]);
                line[k * es] = val;
                if (simp_w) {
                   const double f = (double) dens2(val);
@@ -440,6 +451,22 @@ __global__ void __launch_bounds__(256, kSweepCtas[0]) k_sweep_z(typename Tr<R, C
    P *blk = (P *) (base + S * stage_bytes);
    double *part = (double *) (blk + 2 * (NW + 1) * TR);
    double *part2 = part + tb.P * TR;
+   // FP64: the coefficient tables (alpha, gamma, M, N) staged once per CTA,
+   // the shared rows leaving little L1 for them (z sweep 129 -> 128 us real,
+   // 94 -> 93 us imaginary time at 256^3; FP32 measured slower with it)
+   constexpr bool STAB = std::is_same<R, double>::value;
+   constexpr int TE = CPLX ? 2 : 1;  // doubles per entry
+   double *tabs = part2 + tb.P * TR;
+   SegTab tbs = tb;
+   if constexpr (STAB) {
+      const void *src[4] = {tb.al, tb.ga, tb.M, tb.N};
+      for (int a = 0; a < 4; a++)
+         for (int e = threadIdx.x; e < tb.n * TE; e += blockDim.x) tabs[a * tb.n * TE + e] = ((const double *) src[a])[e];
+      tbs.al = tabs;
+      tbs.ga = tabs + tb.n * TE;
+      tbs.M = tabs + 2 * tb.n * TE;
+      tbs.N = tabs + 3 * tb.n * TE;
+   }
    const int ntiles = (int) ((d.nxy + TR - 1) / TR);
    auto nrows = [&](int t) -> int {
       const long long r0 = (long long) t * TR;
@@ -478,7 +505,7 @@ __global__ void __launch_bounds__(256, kSweepCtas[0]) k_sweep_z(typename Tr<R, C
          __syncthreads();
       }
       double my = 0., my2 = 0.;
-      seg_sweep<R, CPLX, MSEG, TWC>(tile, 1, LS, c, p, TR, tb, blk, SIMP ? wz : nullptr, SIMP ? &my : nullptr,
+      seg_sweep<R, CPLX, MSEG, TWC, NoXf, STAB>(tile, 1, LS, c, p, TR, tbs, blk, SIMP ? wz : nullptr, SIMP ? &my : nullptr,
                                MOM == 2 ? wz2 : nullptr, MOM == 2 ? &my2 : nullptr);
       if (SIMP && p < tb.P) part[p * TR + c] = my;
       if (MOM == 2 && p < tb.P) part2[p * TR + c] = my2;
