@@ -815,7 +815,8 @@ template <class R, bool CPLX> struct Impl {
          const size_t sm = zinv_smem(s, L);
          CKS(with_zrows(L, [&](auto lc) { return zinv_L<decltype(lc)::value>(s, sm); }));
       }
-      CKS(launch_pdl(k_phifix<R>, 256, 256, 0, s, (R *) s->phi, d));
+      CKS(launch_pdl(k_phifix<R>, (unsigned) std::max<long>(1, (d.ny - 1) + (d.nx - 1)),
+                     (unsigned) std::min<long>(256, std::max<long>(32, (d.nz - 1 + 31) / 32 * 32)), 0, s, (R *) s->phi, d));
       CKL();
       mark(s);
       s->launches += 6;

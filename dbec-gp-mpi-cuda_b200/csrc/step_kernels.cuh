@@ -296,23 +296,26 @@ __global__ void __launch_bounds__(256, L >= 16 ? 3 : 4) k_zinv(const cpx<R> *__r
 // imag3d-mpicuda.cu:1591-1625): x = nx-1 <- x = 0 and y = ny-1 <- y = 0 here,
 // each excluding the other two last indices; z = nz-1 <- z = 0 is done inside
 // the rows by k_zinv.  The read and write sets are disjoint, so both copies
-// run concurrently.
+// run concurrently.  One CTA per copied row: blocks [0, ny-1) the rows (nx-1,
+// j) <- (0, j), blocks [ny-1, ny-1 + nx-1) the rows (i, ny-1) <- (i, 0), the
+// first nz-1 points of each (the grid has at least one block).
 template <class R>
 __global__ void k_phifix(R *__restrict__ phi, Dims d) {
    pdl_trigger();
    pdl_wait();
-   const long long A = (long long) (d.ny - 1) * (d.nz - 1);
-   const long long B = (long long) (d.nx - 1) * (d.nz - 1);
-   for (long long e = blockIdx.x * (long long) blockDim.x + threadIdx.x; e < A + B;
-        e += (long long) gridDim.x * blockDim.x) {
-      if (e < A) {
-         const long long j = e / (d.nz - 1), k = e - j * (d.nz - 1);
-         phi[((long long) (d.nx - 1) * d.ny + j) * d.nz + k] = phi[j * d.nz + k];
-      } else {
-         const long long q = e - A, i = q / (d.nz - 1), k = q - i * (d.nz - 1);
-         phi[(i * d.ny + d.ny - 1) * d.nz + k] = phi[(i * d.ny) * d.nz + k];
-      }
+   const int b = blockIdx.x;
+   long long dst, src;
+   if (b < d.ny - 1) {
+      dst = ((long long) (d.nx - 1) * d.ny + b) * d.nz;
+      src = (long long) b * d.nz;
+   } else if (b - (d.ny - 1) < d.nx - 1) {
+      const long long i = b - (d.ny - 1);
+      dst = (i * d.ny + d.ny - 1) * d.nz;
+      src = i * d.ny * d.nz;
+   } else {
+      return;
    }
+   for (int k = threadIdx.x; k < d.nz - 1; k += blockDim.x) phi[dst + k] = phi[src + k];
 }
 
 // ===========================================================================
