@@ -375,7 +375,9 @@ __device__ __forceinline__ double simp_w(int k, int N) {
 // norm = sqrt(S_x S_y rowsum) (calcnorm, imag3d-mpicuda.cu:1194-1218), stores
 // norm, scale = 1/norm and scale^2 in the state.  Each warp forms the
 // weighted Simpson sum over y of one x row (shuffle reduction) into xs[i];
-// the last CTA to finish integrates xs over x.
+// the last CTA to finish integrates xs over x.  The kernel is latency-bound
+// (a few kB of row sums): loads are issued ahead of the sums and the final
+// sum uses the whole CTA (16 -> 10 us at 256^3).
 constexpr int kNormRowsPerCta = 8;
 __global__ void __launch_bounds__(32 * kNormRowsPerCta) k_norm_final(const double *__restrict__ rowsum, Dims d,
                                                                      double hx, double hy, State *st, double *xs,
@@ -385,27 +387,46 @@ __global__ void __launch_bounds__(32 * kNormRowsPerCta) k_norm_final(const doubl
    const int lane = threadIdx.x & 31;
    const int i = blockIdx.x * kNormRowsPerCta + (threadIdx.x >> 5);
    if (i < d.nx) {
+      // a warp per x row; the loads of a lane are issued before the sums
       const double *r = rowsum + (long long) i * d.ny;
-      double a0 = 0., a1 = 0.;
-      int j = lane;
-      for (; j + 32 < d.ny; j += 64) {
-         a0 = fma(simp_w(j, d.ny), r[j], a0);
-         a1 = fma(simp_w(j + 32, d.ny), r[j + 32], a1);
+      constexpr int U = 8;
+      double acc = 0.;
+      for (int j0 = 0; j0 < d.ny; j0 += 32 * U) {
+         double v[U];
+#pragma unroll
+         for (int u = 0; u < U; u++) {
+            const int j = j0 + lane + 32 * u;
+            v[u] = j < d.ny ? r[j] : 0.;
+         }
+#pragma unroll
+         for (int u = 0; u < U; u++) {
+            const int j = j0 + lane + 32 * u;
+            if (j < d.ny) acc = fma(simp_w(j, d.ny), v[u], acc);
+         }
       }
-      if (j < d.ny) a0 = fma(simp_w(j, d.ny), r[j], a0);
-      double acc = a0 + a1;
       for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
       if (lane == 0) xs[i] = acc * hy / 3.;
    }
    __threadfence();
    __syncthreads();
    __shared__ bool last;
+   __shared__ double red[32 * kNormRowsPerCta];
    if (threadIdx.x == 0) last = atomicAdd(&st->ticket, 1u) == gridDim.x - 1;
    __syncthreads();
-   if (!last || threadIdx.x >= 32) return;
+   if (!last) return;
+   // last CTA: every thread takes its strided share of the x rows, then a
+   // fixed-order tree over the CTA
    __threadfence();
    double acc = 0.;
-   for (int k = lane; k < d.nx; k += 32) acc = fma(simp_w(k, d.nx), __ldcg(xs + k), acc);
+   for (int k = threadIdx.x; k < d.nx; k += blockDim.x) acc = fma(simp_w(k, d.nx), __ldcg(xs + k), acc);
+   red[threadIdx.x] = acc;
+   __syncthreads();
+   for (int h = blockDim.x / 2; h >= 32; h >>= 1) {
+      if ((int) threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+      __syncthreads();
+   }
+   if (threadIdx.x >= 32) return;
+   acc = red[threadIdx.x];
    for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
    if (lane == 0) {
       const double nrm = sqrt(acc * hx / 3.);
