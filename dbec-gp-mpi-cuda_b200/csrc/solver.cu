@@ -711,9 +711,10 @@ template <class R, bool CPLX> struct Impl {
    }
    // points per thread of the z passes: (nz/2) L over 256 threads
    static int zppt(const gpe_solver *s, int L) { return (int) (((s->d.nz / 2) * L + 255) / 256); }
-   // threads of a z inverse pass CTA: PPT points each of the L half-length
-   // lines (the forward pass keeps 256: sized CTAs measured slower there,
-   // 101 -> 105 us at 256^3 complex FP64)
+   // threads of a z inverse pass CTA, and of a forward pass CTA over real
+   // FP32 rows: PPT points each of the L half-length lines (the other forward
+   // passes keep 256: sized CTAs measured slower there, 101 -> 105 us at
+   // 256^3 complex FP64)
    static unsigned z_threads(const gpe_solver *s, int L, int ppt) {
       const long t = ((long) (s->d.nz / 2) * L + ppt - 1) / ppt;
       return (unsigned) std::min<long>(256, std::max<long>(32, (t + 31) / 32 * 32));
@@ -757,7 +758,8 @@ template <class R, bool CPLX> struct Impl {
       return with_ppt(zppt(s, L), [&](auto pc) {
          constexpr int PPT = decltype(pc)::value;
          CKS(smem_attr((const void *) k_zfwd<R, CPLX, PPT, L>, sm));
-         CKS(launch_pdl(k_zfwd<R, CPLX, PPT, L>, blocks_for(d.nxy, L), 256, sm, s, (const P *) s->psi, (C *) s->spec, d,
+         const unsigned nt = (sizeof(R) == 4 && !CPLX) ? z_threads(s, L, PPT) : 256u;
+         CKS(launch_pdl(k_zfwd<R, CPLX, PPT, L>, blocks_for(d.nxy, L), nt, sm, s, (const P *) s->psi, (C *) s->spec, d,
                         s->ph, (const C *) s->twz, s->LSr, s->err));
          CKL();
          mark(s);
