@@ -712,9 +712,9 @@ template <class R, bool CPLX> struct Impl {
    // points per thread of the z passes: (nz/2) L over 256 threads
    static int zppt(const gpe_solver *s, int L) { return (int) (((s->d.nz / 2) * L + 255) / 256); }
    // threads of a z inverse pass CTA, and of a forward pass CTA over real
-   // FP32 rows: PPT points each of the L half-length lines (the other forward
-   // passes keep 256: sized CTAs measured slower there, 101 -> 105 us at
-   // 256^3 complex FP64)
+   // rows: PPT points each of the L half-length lines (the forward passes
+   // over complex rows keep 256: sized CTAs measured slower there, 101 -> 105
+   // us at 256^3 complex FP64)
    static unsigned z_threads(const gpe_solver *s, int L, int ppt) {
       const long t = ((long) (s->d.nz / 2) * L + ppt - 1) / ppt;
       return (unsigned) std::min<long>(256, std::max<long>(32, (t + 31) / 32 * 32));
@@ -753,12 +753,12 @@ template <class R, bool CPLX> struct Impl {
    }
 
    // z pass kernels for a tile of L rows
-   template <int L> static gpe_status zfwd_L(gpe_solver *s, size_t sm) {
+   template <int L> static gpe_status zfwd_L(gpe_solver *s, size_t sm, bool sized) {
       const Dims &d = s->d;
       return with_ppt(zppt(s, L), [&](auto pc) {
          constexpr int PPT = decltype(pc)::value;
          CKS(smem_attr((const void *) k_zfwd<R, CPLX, PPT, L>, sm));
-         const unsigned nt = (sizeof(R) == 4 && !CPLX) ? z_threads(s, L, PPT) : 256u;
+         const unsigned nt = sized ? z_threads(s, L, PPT) : 256u;
          CKS(launch_pdl(k_zfwd<R, CPLX, PPT, L>, blocks_for(d.nxy, L), nt, sm, s, (const P *) s->psi, (C *) s->spec, d,
                         s->ph, (const C *) s->twz, s->LSr, s->err));
          CKL();
@@ -805,9 +805,13 @@ template <class R, bool CPLX> struct Impl {
    static gpe_status psidd2(gpe_solver *s) {
       const Dims &d = s->d;
       {
-         const int L = zrows(s, ZRows<R, CPLX>::fwd, zfwd_smem);
+         // real rows: 8-row tiles on CTAs sized to them, except FP64 rows
+         // shorter than 128 points, which keep 16 rows on 256 threads (sized
+         // CTAs of 32 threads measured slower at 64^3: 8.8 -> 10.8 us)
+         const bool sized = !CPLX && (sizeof(R) == 4 || d.nz >= 128);
+         const int L = zrows(s, (!CPLX && !sized) ? 16 : ZRows<R, CPLX>::fwd, zfwd_smem);
          const size_t sm = zfwd_smem(s, L);
-         CKS(with_zrows(L, [&](auto lc) { return zfwd_L<decltype(lc)::value>(s, sm); }));
+         CKS(with_zrows(L, [&](auto lc) { return zfwd_L<decltype(lc)::value>(s, sm, sized); }));
       }
       CKS(with_L(s->Ly, [&](auto Lc) { return yfft<false, decltype(Lc)::value>(s); }));
       CKS(with_L(s->Lx, [&](auto Lc) { return xconv<decltype(Lc)::value>(s); }));

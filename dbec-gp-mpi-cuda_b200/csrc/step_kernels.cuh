@@ -29,17 +29,18 @@ template <class R> struct FftL {
    static constexpr int PPT = sizeof(R) == 8 ? 8 : 16;
 };
 
-// Preferred rows per CTA of the z passes.  Forward: 16, so that the radix-8
-// stages (nz/2-point lines) keep all 256 threads busy, except over complex
-// FP64 rows (4 KB each), which measured faster with 8 rows and four CTAs per
-// SM, and over real FP32 rows, which measured faster with 8 rows on a CTA
-// sized to them (128 threads at nz = 256; 512x512x256 280 -> 238 us).
+// Preferred rows per CTA of the z passes.  Forward: 16 over complex FP32
+// rows, so that the radix-8 stages (nz/2-point lines) keep all 256 threads
+// busy; 8 over complex FP64 rows (4 KB each), which measured faster with four
+// CTAs per SM; 8 over real rows on a CTA sized to them (128 threads at nz =
+// 256; 512x512x256 FP32 280 -> 238 us, 256^3 FP64 93 -> 87 us), where the
+// host keeps 16 rows on 256 threads for FP64 rows shorter than 128 points.
 // Inverse: 8 rows on a CTA sized to them (128 threads at nz = 256), six
 // per SM, measured faster than 16 rows on 256 threads (256^3 FP64 82 -> 78
 // us, 512x512x256 FP32 238 -> 210 us).  The host halves the rows while the
 // tile does not fit shared memory.
 template <class R, bool CPLX> struct ZRows {
-   static constexpr int fwd = (sizeof(R) == 8 && CPLX) || (sizeof(R) == 4 && !CPLX) ? 8 : 16;
+   static constexpr int fwd = (sizeof(R) == 4 && CPLX) ? 16 : 8;
    static constexpr int inv = 8;
 };
 
