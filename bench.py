@@ -13,6 +13,12 @@ every 100 steps.  A "step" is one full split step over the 256^3 grid
   e2e    the same metric through the C ABI with host buffers: psi copied
          from page-locked host memory, K steps with rms every 100 steps,
          psi copied back, all inside the timed region
+The default line also carries the headline comparison of the metric
+(`baseline_metric`: the mixed-precision imaginary-time step at 256^3 against
+the plain FP64 step on the same box, with the mixed result's |dmu/mu| and
+density L2 error against the FP64 run after the same steps) and `cufft_ab`,
+the dipolar convolution timed through cuFFT against the solver's own passes.
+--workload mixed256 prints that comparison as its own line;
 --workload mixed512 measures the mixed-precision imaginary-time step at
 512x512x256 instead (FP32 / complex64 bulk, FP64 reductions and tables);
 --workload batched64 the 64-instance mixed-precision batch (one CUDA graph per
@@ -51,6 +57,14 @@ WORKLOADS = {
                      desc="imaginary-time dipolar GP, mixed precision (FP32 psi/FFT/sweeps, FP64 norm and tables), "
                           "512x512x256, dx=0.25, dt=6.25e-3, trap (0.5,1,1.5), g=100, gd=30, R=32",
                      metric="grid-pt-steps/s (mixed-precision imaginary-time step, 512x512x256)",
+                     b_min=8 * 4 + 8 * (129 / 256) * 8 + (129 / 256) * 8),
+    "mixed256": dict(mode=0, precision=1, grid=(256, 256, 256), dx=0.2, dt=0.1 * 0.2 * 0.2, trap=(1.0, 1.0, 4.0),
+                     g=200.0, gd=60.0, dtype="f32 (FP64 reductions)", psi_bytes=4,
+                     desc="imaginary-time dipolar GP, mixed precision (FP32 psi/FFT/sweeps, FP64 norm and tables), "
+                          "256^3, dx=0.2, dt=4e-3, trap (1,1,4), g=200, gd=60, R=25.6 (the ground-state half of "
+                          "the 256^3 configuration), against the plain FP64 step",
+                     metric="grid-pt-steps/s vs plain FP64 at |dmu/mu|<=1e-6 (mixed-precision imaginary-time step, "
+                            "256^3)",
                      b_min=8 * 4 + 8 * (129 / 256) * 8 + (129 / 256) * 8),
     "batched64": dict(desc="64 independent imaginary-time solves, mixed precision, grids drawn from {48^3, 64^3, "
                            "96x96x64, 128^3}, g~U[20,400], gd~U[0,0.9g], gamma,nu~U[0.5,2], lambda~U[0.5,8], "
@@ -396,6 +410,129 @@ def run_serving(args, wl):
     return 0
 
 
+def arm_config(wl, world):
+    """The `config` object of a single-solve line, identical in both arms."""
+    nx, ny, nz = wl["grid"]
+    return {"workload": wl["desc"], "grid": list(wl["grid"]),
+            "precision": "fp64" if wl["precision"] == 0 else "mixed",
+            "parallelism": "replicas x%d" % world,
+            "l2": "inputs larger than L2 (psi %d MB), no flush" % (nx * ny * nz * wl["psi_bytes"] // 1000000)}
+
+
+def make_solver(wl, local, precision=None):
+    import gpe
+    nx, ny, nz = wl["grid"]
+    dx = wl["dx"]
+    prec = wl["precision"] if precision is None else precision
+    p = gpe.make_params(wl["mode"], nx, ny, nz, dx, dx, dx, wl["dt"], *wl["trap"], cutoff_of(wl), opt=1,
+                        precision=prec, device=local)
+    return gpe.Solver(p), p
+
+
+def mixed_vs_plain(K, W, local, accuracy_steps):
+    """The headline comparison of the metric at 256^3: device-timed
+    grid-pt-steps/s of the mixed-precision imaginary-time step and of the
+    plain FP64 step on this GPU, and the mixed result's error against the FP64
+    run after `accuracy_steps` renormalised steps from the same Gaussian."""
+    import numpy as np
+    wl = WORKLOADS["mixed256"]
+    npts = int(np.prod(wl["grid"]))
+    G, GD = wl["g"], wl["gd"]
+    res = {}
+    for prec in (0, 1):
+        s, _ = make_solver(wl, local, precision=prec)
+        s.init_gaussian()
+        s.calcnorm(True)
+        s.time_steps(W, G, GD)
+        ms = s.time_steps(K, G, GD)
+        s.init_gaussian()
+        s.calcnorm(True)
+        _, _, last_norm, _ = s.run(accuracy_steps, G, GD)
+        mu, en = s.calcmuen(G, GD)
+        res[prec] = dict(ms=ms / K, value=npts * K / (ms / 1e3), mu=mu, en=en, norm=last_norm, rms=s.calcrms(),
+                         rho=np.abs(s.get_psi()) ** 2)
+        s.close()
+    a, b = res[1], res[0]
+    den_l2 = float(np.linalg.norm((a["rho"] - b["rho"]).ravel()) / np.linalg.norm(b["rho"].ravel()))
+    return {"workload": "mixed256", "grid": list(wl["grid"]),
+            "mixed_grid_pt_steps_per_s": a["value"], "mixed_ms_per_step": a["ms"],
+            "plain_fp64_grid_pt_steps_per_s": b["value"], "plain_fp64_ms_per_step": b["ms"],
+            "vs_plain_fp64": a["value"] / b["value"],
+            "accuracy_steps": accuracy_steps, "dmu_rel": abs(a["mu"] / b["mu"] - 1),
+            "en_rel": abs(a["en"] / b["en"] - 1), "rms_rel": float(np.max(np.abs(a["rms"] - b["rms"]) / np.abs(b["rms"]))),
+            "norm_rel": abs(a["norm"] / b["norm"] - 1), "density_l2_rel": den_l2,
+            "meets_dmu_1e-6": abs(a["mu"] / b["mu"] - 1) <= 1e-6}
+
+
+def cufft_ab(wl, local, nrep=10):
+    """The dipolar convolution of this workload through cuFFT (the reference's
+    call structure, and one batched plan per direction) against the solver's
+    own five FFT passes plus boundary planes, on the same psi."""
+    import numpy as np
+    import gpe
+    s, p = make_solver(wl, local)
+    s.init_gaussian()
+    own_ms = s.time_calcpsidd2(nrep)
+    s.calcpsidd2()
+    own_phi = s.get_phi()
+    psi = s.get_psi()
+    s.close()
+    out = {"grid": list(wl["grid"]), "precision": "fp64" if wl["precision"] == 0 else "mixed (FP32 cuFFT)",
+           "own_ms": own_ms}
+    for variant, key in ((0, "cufft_reference_structure"), (1, "cufft_batched")):
+        phi, ms = gpe.cufft_convolution(p, psi, variant=variant, nrep=3 if variant == 0 else nrep)
+        out[key + "_ms"] = ms
+        out[key + "_phi_rel_diff"] = float(np.max(np.abs(phi - own_phi)) / np.max(np.abs(own_phi)))
+    out["own_speedup_vs_cufft_batched"] = out["cufft_batched_ms"] / own_ms
+    out["own_speedup_vs_cufft_reference_structure"] = out["cufft_reference_structure_ms"] / own_ms
+    out["note"] = ("CUDA events, mean of %d convolutions after one warm-up; cuFFT plans and buffers made outside the "
+                   "timed region; variant 0 = D2Z, one-rank transpose copy, one Z2Z per y line, Udd multiply, "
+                   "inverse, copy back, Z2D, boundary planes (imag3d-mpicuda.cu:1460-1510)" % nrep)
+    return out
+
+
+def run_reference(args, wl, K, W, world):
+    """The reference's CPU path: the FP64 restatement of the reference step
+    (oracle/, OpenMP over all host cores) on this workload, W untimed and K
+    timed whole steps (a time cap stops it early and the line says so)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    oracle.build()
+    cores = os.cpu_count() or 1
+    oracle.set_threads(cores)
+    nx, ny, nz = wl["grid"]
+    dx = wl["dx"]
+    o = oracle.Oracle(wl["mode"], 1, nx, ny, nz, dx, dx, dx, wl["dt"], *wl["trap"], cutoff_of(wl))
+    o.init_gaussian()
+    cap_s = 240.0
+    t0 = time.perf_counter()
+    w = 0
+    while w < W and time.perf_counter() - t0 < cap_s / 4:
+        o.run(1, wl["g"], wl["gd"])
+        w += 1
+    t0 = time.perf_counter()
+    n = 0
+    while n < K:
+        o.run(1, wl["g"], wl["gd"])
+        n += 1
+        if time.perf_counter() - t0 > cap_s:
+            break
+    dt = time.perf_counter() - t0
+    o.close()
+    v = nx * ny * nz * n / dt
+    line = {"impl": "reference", "metric": wl["metric"], "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": n,
+            "warmup": w, "ms_per_step": 1e3 * dt / n, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (deterministic Gaussian initial state)",
+            "config": arm_config(wl, world),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": "%d untimed + %d timed whole steps of this workload on the FP64 CPU "
+                                       "restatement of the reference step (OpenMP, %d threads), %.1f s timed"
+                                       % (w, n, cores, dt)},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -404,6 +541,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="real256", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--accuracy-steps", type=int, default=2000,
+                    help="renormalised steps before the mixed-vs-FP64 error comparison")
     args = ap.parse_args()
     K, W = args.steps, max(3, args.warmup)
     wl = WORKLOADS[args.workload]
@@ -413,7 +552,7 @@ def main():
         return run_batched(args, wl) if args.workload == "batched64" else run_serving(args, wl)
     if "grid" not in wl:
         print(json.dumps({"impl": "reference", "unavailable": "the CPU restatement times single solves; use the "
-                          "real256 or mixed512 workloads for the reference arm"}), flush=True)
+                          "real256, mixed256 or mixed512 workloads for the reference arm"}), flush=True)
         return 0
     nx, ny, nz = wl["grid"]
     npts = nx * ny * nz
@@ -426,20 +565,9 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        v, cores, n, dt = cpu_reference(wl, steps_cap=max(1, min(K, cpu_steps)))
-        line = {"impl": "reference", "metric": wl["metric"], "value": v, "unit": UNIT, "n_gpus": args.gpus,
-                "steps": K, "warmup": W, "ms_per_step": 1e3 * dt / n, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic (deterministic Gaussian initial state)",
-                "config": {"workload": wl["desc"], "grid": list(wl["grid"]), "timed_steps": n},
-                "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                                 "sample": "%d whole step(s) of this workload on the FP64 CPU restatement of the "
-                                           "reference step (OpenMP, %d threads), %.1f s" % (n, cores, dt)},
-                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
-        return 0
+        return run_reference(args, wl, K, W, world)
 
     import torch
-    import gpe
 
     torch.cuda.set_device(local)
     dist = None
@@ -448,10 +576,7 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
-    dx = wl["dx"]
-    p = gpe.make_params(wl["mode"], nx, ny, nz, dx, dx, dx, wl["dt"], *wl["trap"], cutoff_of(wl), opt=1,
-                        precision=wl["precision"], device=local)
-    s = gpe.Solver(p)
+    s, p = make_solver(wl, local)
     s.init_gaussian()
     G, GD = wl["g"], wl["gd"]
     s.time_steps(W, G, GD)  # warm-up
@@ -512,6 +637,13 @@ def main():
                    "wall clock"}
     s.close()
 
+    extra = {}
+    if rank == 0 and world == 1:
+        if args.workload in ("real256", "mixed256"):
+            extra["baseline_metric"] = mixed_vs_plain(K, W, local, args.accuracy_steps)
+        if args.workload in ("real256", "mixed512"):
+            extra["cufft_ab"] = cufft_ab(wl, local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, cores, n, dt = cpu_reference(wl, steps_cap=cpu_steps)
@@ -520,15 +652,18 @@ def main():
                          "(OpenMP, %d threads), %.1f s" % (n, cores, dt)}
 
     if rank == 0:
+        cfg = arm_config(wl, world)
         line = {"metric": wl["metric"], "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
                 "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": wl["dtype"], "data": "synthetic (deterministic Gaussian initial state; per-step work is "
                                               "independent of the state)",
-                "config": {"workload": wl["desc"], "grid": list(wl["grid"]),
-                           "precision": "fp64" if wl["precision"] == 0 else "mixed",
-                           "parallelism": "replicas x%d" % world,
-                           "l2": "inputs larger than L2 (psi %d MB), no flush" % (bytes_psi // 1000000)},
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk}
+                "config": cfg, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clk}
+        if args.workload == "mixed256":
+            bm = extra["baseline_metric"] if "baseline_metric" in extra else None
+            line["vs_plain_fp64"] = bm["vs_plain_fp64"] if bm else None
+            line["dmu_rel"] = bm["dmu_rel"] if bm else None
+        line.update(extra)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

@@ -2,6 +2,7 @@
 
 Compiles, for sm_100a only:
   lib/libgpe.so            C ABI (include/gpe.h): kernels + handle
+  lib/libgpe_cufft.so      cuFFT convolution kept as a timed comparison (include/gpe_cufft.h)
   bin/imag3d-mpicuda       drop-in CLI for imaginary time
   bin/real3d-mpicuda       drop-in CLI for real time
 Uses nvcc directly (no torch extension): the library has no torch types in
@@ -34,6 +35,10 @@ HOST_COMMON = ["cfg.cpp", "cli.cpp"]
 PROGRAMS = {"imag3d-mpicuda": "imag3d_main.cpp", "real3d-mpicuda": "real3d_main.cpp"}
 
 LIB = os.path.join(LIB_DIR, "libgpe.so")
+# the cuFFT pipeline kept only as a timed comparison: its own library, so the
+# solver itself never links cuFFT
+CUFFT_SOURCES = ["cufft_compare.cu"]
+CUFFT_LIB = os.path.join(LIB_DIR, "libgpe_cufft.so")
 
 
 def _stale(target, deps):
@@ -58,6 +63,16 @@ def build_lib(force=False, verbose_ptxas=False):
     return LIB
 
 
+def build_cufft_lib(force=False):
+    os.makedirs(LIB_DIR, exist_ok=True)
+    deps = [os.path.join(CSRC, f) for f in CUFFT_SOURCES] + [os.path.join(INCLUDE, "gpe.h"),
+                                                             os.path.join(INCLUDE, "gpe_cufft.h")]
+    if force or _stale(CUFFT_LIB, deps):
+        _run([NVCC] + NVFLAGS + ["-shared", "-o", CUFFT_LIB] + [os.path.join(CSRC, f) for f in CUFFT_SOURCES] +
+             ["-lcufft", "-lcudart"])
+    return CUFFT_LIB
+
+
 def build_programs(force=False):
     os.makedirs(BIN_DIR, exist_ok=True)
     out = {}
@@ -75,6 +90,7 @@ def build_programs(force=False):
 
 def build(force=False):
     build_lib(force)
+    build_cufft_lib(force)
     if os.path.exists(os.path.join(HOST, "cli.cpp")):
         build_programs(force)
     return LIB

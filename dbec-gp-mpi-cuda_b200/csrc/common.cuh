@@ -103,6 +103,20 @@ struct Simpson {
    }
 };
 
+// Weight of sample k in simpint over N samples (src/utils/diffint.cu:37-66),
+// in units of h/3: 1, 4, 2, ..., 4, 1 over the first odd count of samples,
+// plus the end correction (5 f[N-1] + 8 f[N-2] - f[N-3]) / 4 for even N.
+__host__ __device__ __forceinline__ double simp_w(int k, int N) {
+   const int mm = (N & 1) ? N : N - 1;
+   double w = k < mm ? ((k == 0 || k == mm - 1) ? 1. : ((k & 1) ? 4. : 2.)) : 0.;
+   if (!(N & 1)) {
+      if (k == N - 1) w += 1.25;
+      else if (k == N - 2) w += 2.;
+      else if (k == N - 3) w -= 0.25;
+   }
+   return w;
+}
+
 // Simpson over an array in memory, the reference's loop verbatim in order.
 __host__ __device__ __forceinline__ double simpint_arr(double h, const double *f, long N, long st = 1) {
    double sumi = 0., sumj = 0., sumk = 0.;

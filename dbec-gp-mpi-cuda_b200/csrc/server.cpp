@@ -30,6 +30,7 @@
 #include <deque>
 #include <map>
 #include <mutex>
+#include <set>
 #include <string>
 #include <thread>
 #include <vector>
@@ -52,6 +53,7 @@ struct Active {
    gpe_status st = GPE_OK;
    bool done = false;
    bool inflight = false;
+   bool cancel = false;  // gpe_server_cancel: retire at the next chunk boundary
    cudaEvent_t ev = nullptr;
    cudaStream_t stream = nullptr;  // created by the server with a priority
 };
@@ -84,6 +86,7 @@ struct gpe_server {
    std::condition_variable cv_work, cv_done;
    std::deque<Pending> queue;
    std::map<long long, gpe_result> results;
+   std::set<long long> cancel_req;  // ids of admitted requests to cancel
    long long next_id = 1;
    bool stopping = false;
    double stats[4] = {0, 0, 0, 0};
@@ -99,7 +102,8 @@ struct gpe_server {
       r.t_submit = a.t_submit;
       r.t_start = a.t_start;
       r.mu = r.en = r.norm = NAN;
-      if (a.st == GPE_OK) {
+      if (a.cancel && a.st == GPE_OK) r.status = GPE_ERR_CANCELLED;
+      if (a.st == GPE_OK && !a.cancel) {
          gpe_status st = gpe::queue_muen(a.s, a.rq.g, a.rq.gd);
          if (st == GPE_OK) st = gpe::read_muen(a.s, &r.mu, &r.en);
          if (st == GPE_OK) st = gpe_calcnorm(a.s, 0, &r.norm);
@@ -115,6 +119,7 @@ struct gpe_server {
       r.t_done = now();
       std::lock_guard<std::mutex> lk(mu);
       results[a.id] = r;
+      cancel_req.erase(a.id);
       stats[0] += 1;
       cv_done.notify_all();
    }
@@ -196,6 +201,7 @@ struct gpe_server {
                r.t_done = now();
                std::lock_guard<std::mutex> lk(mu);
                results[a.id] = r;
+               cancel_req.erase(a.id);
                stats[0] += 1;
                cv_done.notify_all();
                continue;
@@ -209,6 +215,15 @@ struct gpe_server {
             stats[2] = std::max(stats[2], (double) used);
          }
          if (active.empty()) continue;
+         // cancellations: a solve stops at its next chunk boundary (never with
+         // a chunk of its kernels in flight)
+         {
+            std::lock_guard<std::mutex> lk(mu);
+            for (Active &a : active)
+               if (cancel_req.count(a.id)) a.cancel = true;
+         }
+         for (Active &a : active)
+            if (a.cancel && !a.inflight) a.done = true;
          // 2. next chunks, least remaining work first, within the fill budget
          long long fill = 0;
          for (const Active &a : active)
@@ -265,7 +280,7 @@ struct gpe_server {
             } else {
                a.st = gpe_synchronize(a.s);
             }
-            if (a.steps >= a.rq.max_steps || a.st != GPE_OK) a.done = true;
+            if (a.steps >= a.rq.max_steps || a.st != GPE_OK || a.cancel) a.done = true;
          }
          for (Active &a : active)
             if (a.done && !a.inflight) {
@@ -337,6 +352,30 @@ extern "C" gpe_status gpe_server_wait(gpe_server *sv, long long id, double timeo
       return sfail(GPE_ERR_TIMEOUT, "server: request not finished in time");
    }
    if (res) *res = sv->results[id];
+   return GPE_OK;
+}
+
+extern "C" gpe_status gpe_server_cancel(gpe_server *sv, long long id) {
+   if (!sv) return sfail(GPE_ERR_PARAM, "server: null handle");
+   std::lock_guard<std::mutex> lk(sv->mu);
+   if (id < 1 || id >= sv->next_id) return sfail(GPE_ERR_PARAM, "server: unknown request id");
+   if (sv->results.count(id)) return sfail(GPE_ERR_STATE, "server: request already finished");
+   for (auto it = sv->queue.begin(); it != sv->queue.end(); ++it)
+      if (it->id == id) {
+         // still queued: never admitted, nothing on the device
+         gpe_result r{};
+         r.id = id;
+         r.status = GPE_ERR_CANCELLED;
+         r.mu = r.en = r.norm = NAN;
+         r.t_submit = it->t_submit;
+         r.t_start = r.t_done = sv->now();
+         sv->queue.erase(it);
+         sv->results[id] = r;
+         sv->stats[0] += 1;
+         sv->cv_done.notify_all();
+         return GPE_OK;
+      }
+   sv->cancel_req.insert(id);  // admitted: the worker retires it at the next chunk boundary
    return GPE_OK;
 }
 

@@ -83,6 +83,8 @@ struct gpe_solver {
    double *x2 = nullptr, *y2 = nullptr, *z2 = nullptr;
    void *lin[3] = {nullptr, nullptr, nullptr};  // per-axis trap factors of calcnu, imag (LinPhase)
    double *rowA = nullptr, *rowB = nullptr, *tmp = nullptr, *obs = nullptr;
+   double *rms_buf = nullptr;  // rms samples of gpe_run, kRmsSlots x 4 doubles
+
    long long row_cap = 0;  // doubles in rowA / rowB: the largest of nx*ny, nx*nz, ny*nz
    State *state = nullptr;
    std::vector<double> hx, hy, hz, hx2, hy2, hz2;
@@ -105,6 +107,10 @@ struct gpe_solver {
    cudaEvent_t *prof_ev = nullptr;
    int prof_i = 0, prof_cap = 0;
 };
+
+// rms samples gpe_run keeps on the device before copying them out (a run with
+// more samples copies every full batch of slots while it continues)
+constexpr long kRmsSlots = 256;
 
 static void mark(gpe_solver *s) {
    if (s->prof_ev && s->prof_i < s->prof_cap) cudaEventRecord(s->prof_ev[s->prof_i++], s->st);
@@ -530,7 +536,7 @@ static gpe_status make_udd(gpe_solver *s) {
 
 static void free_all(gpe_solver *s) {
    void *ptrs[] = {s->psi, s->spec, s->phi, s->twx, s->twy, s->twz, s->udd, s->x2, s->y2, s->z2,
-                   s->rowA, s->rowB, s->tmp, s->obs, s->state};
+                   s->rowA, s->rowB, s->tmp, s->obs, s->state, s->rms_buf};
    for (void *q : ptrs)
       if (q) cudaFree(q);
    for (int a = 0; a < 3; a++) {
@@ -583,6 +589,7 @@ static gpe_status create_impl(const gpe_params *p, void *stream, gpe_solver *s) 
    CK(cudaMalloc(&s->tmp, sizeof(double) * std::max<long long>(d.nxy, std::max(d.nx, std::max(d.ny, d.nz))) * 2));
    s->obs_cap = 64;
    CK(cudaMalloc(&s->obs, sizeof(double) * s->obs_cap));
+   CK(cudaMalloc(&s->rms_buf, sizeof(double) * 4 * kRmsSlots));
    CK(cudaMalloc(&s->state, sizeof(State)));
    State st0{};
    st0.norm = 1.; st0.scale = 1.; st0.scale2 = 1.;
@@ -1231,39 +1238,46 @@ extern "C" gpe_status gpe_run(gpe_solver *s, long nsteps, double *g, double *gd,
    if (nsteps < 0) return fail(GPE_ERR_PARAM, "negative step count");
    CK(cudaSetDevice(s->dev));
    const bool imag = !s->cplx;
-   long nrms = (rms_every > 0) ? (nsteps + rms_every - 1) / rms_every : 0;
-   double *drms = nullptr;
-   if (nrms > 0) {
-      if (!rms_out) return fail(GPE_ERR_PARAM, "rms_out required when rms_every > 0");
-      CK(cudaMalloc(&drms, sizeof(double) * 4 * nrms));
-   }
+   const long nrms = (rms_every > 0) ? (nsteps + rms_every - 1) / rms_every : 0;
+   if (nrms > 0 && !rms_out) return fail(GPE_ERR_PARAM, "rms_out required when rms_every > 0");
+   // rms samples land in the handle's preallocated slots (no allocation and
+   // no implicit synchronisation inside the run); every kRmsSlots samples the
+   // full batch is copied out
+   long flushed = 0;  // samples already copied to rms_out
+   auto flush = [&](long upto) -> gpe_status {
+      if (upto <= flushed) return GPE_OK;
+      CK(cudaMemcpyAsync(rms_out + 4 * flushed, s->rms_buf, sizeof(double) * 4 * (upto - flushed),
+                         cudaMemcpyDeviceToHost, s->st));
+      CK(cudaStreamSynchronize(s->st));
+      flushed = upto;
+      return GPE_OK;
+   };
    gpe_status st = GPE_OK;
    for (long c = 0; c < nsteps && st == GPE_OK; c++) {
       *g += g_inc;
       *gd += gd_inc;
       const bool rms_here = rms_every > 0 && c % rms_every == 0;
+      double *slot = nullptr;
+      if (rms_here) {
+         const long idx = c / rms_every;
+         if (idx - flushed == kRmsSlots) st = flush(idx);
+         slot = s->rms_buf + 4 * (idx - flushed);
+      }
       // real time: the step's z sweep leaves the rms row partials (no extra
       // pass over psi); imaginary time: renormalise first, then a full rms
-      st = DISPATCH(s, step(s, *g, *gd, s->obs, rms_here && !imag));
+      if (st == GPE_OK) st = DISPATCH(s, step(s, *g, *gd, s->obs, rms_here && !imag));
       if (st == GPE_OK && rms_here) {
          if (imag) {
             st = DISPATCH(s, apply_scale(s));
-            if (st == GPE_OK) st = DISPATCH(s, rms(s, drms + 4 * (c / rms_every)));
+            if (st == GPE_OK) st = DISPATCH(s, rms(s, slot));
          } else {
-            st = DISPATCH(s, rms_final(s, drms + 4 * (c / rms_every)));
+            st = DISPATCH(s, rms_final(s, slot));
          }
       }
    }
    if (st == GPE_OK && imag && nsteps > 0) st = DISPATCH(s, apply_scale(s));
    if (st == GPE_OK && last_norm && imag && nsteps > 0) st = read_obs(s, last_norm, 1);
-   if (drms) {
-      if (st == GPE_OK) {
-         cudaError_t e = cudaMemcpyAsync(rms_out, drms, sizeof(double) * 4 * nrms, cudaMemcpyDeviceToHost, s->st);
-         if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
-         if (e != cudaSuccess) st = fail(GPE_ERR_CUDA, cudaGetErrorString(e));
-      }
-      cudaFree(drms);
-   }
+   if (st == GPE_OK && nrms > 0) st = flush(nrms);
    if (st == GPE_OK) {
       cudaError_t e = cudaStreamSynchronize(s->st);
       if (e != cudaSuccess) st = fail(GPE_ERR_CUDA, cudaGetErrorString(e));
@@ -1373,6 +1387,16 @@ extern "C" gpe_status gpe_synchronize(gpe_solver *s) {
    return check_err(s);
 }
 
+extern "C" gpe_status gpe_selftest_wait_timeout(gpe_solver *s, unsigned spins) {
+   CHECK_HANDLE(s);
+   if (spins < 1 || spins > (1u << 16)) return fail(GPE_ERR_PARAM, "spins must be in [1, 65536]");
+   CK(cudaSetDevice(s->dev));
+   k_wait_selftest<<<1, 32, 0, s->st>>>(spins, s->err);
+   CKL();
+   s->launches++;
+   return GPE_OK;
+}
+
 extern "C" gpe_status gpe_launch_count(gpe_solver *s, long long *count) {
    CHECK_HANDLE(s);
    if (count) *count = s->launches;
@@ -1396,6 +1420,28 @@ extern "C" gpe_status gpe_time_steps(gpe_solver *s, long nsteps, double g, doubl
    cudaEventDestroy(a);
    cudaEventDestroy(b);
    if (ms) *ms = f;
+   return st;
+}
+
+extern "C" gpe_status gpe_time_calcpsidd2(gpe_solver *s, long nrep, double *ms) {
+   CHECK_HANDLE(s);
+   if (nrep < 1) return fail(GPE_ERR_PARAM, "nrep must be >= 1");
+   CK(cudaSetDevice(s->dev));
+   CKS(DISPATCH(s, psidd2(s)));  // untimed warm-up
+   cudaEvent_t a, b;
+   CK(cudaEventCreate(&a));
+   CK(cudaEventCreate(&b));
+   CK(cudaEventRecord(a, s->st));
+   gpe_status st = GPE_OK;
+   for (long c = 0; c < nrep && st == GPE_OK; c++) st = DISPATCH(s, psidd2(s));
+   CK(cudaEventRecord(b, s->st));
+   CK(cudaEventSynchronize(b));
+   float f = 0;
+   CK(cudaEventElapsedTime(&f, a, b));
+   cudaEventDestroy(a);
+   cudaEventDestroy(b);
+   if (ms) *ms = f / nrep;
+   if (st == GPE_OK) st = check_err(s);
    return st;
 }
 

@@ -321,6 +321,22 @@ __global__ void k_phifix(R *__restrict__ phi, Dims d) {
    for (int k = threadIdx.x; k < d.nz - 1; k += blockDim.x) phi[dst + k] = phi[src + k];
 }
 
+// Self-test of the bounded waits: one CTA waits on an mbarrier that expects
+// 16 bytes of a transaction no copy will ever deliver.  No copy is issued, so
+// nothing is in flight when the wait gives up after `spins` polls; the CTA
+// then leaves together, exactly as a step kernel whose tile never arrived,
+// and the handle's status word reports the timeout.
+__global__ void k_wait_selftest(uint32_t spins, uint32_t *err) {
+   __shared__ __align__(8) uint64_t bar;
+   if (threadIdx.x == 0) {
+      mbar_init(&bar, 1);
+      fence_mbar_init();
+   }
+   __syncthreads();
+   if (threadIdx.x == 0) mbar_arrive_expect_tx(&bar, 16u);
+   if (__syncthreads_or(!mbar_wait_n(&bar, 0, err, spins))) return;
+}
+
 // ===========================================================================
 // Sweeps.
 // ===========================================================================
@@ -359,20 +375,6 @@ __global__ void k_rows_dens(const typename Tr<R, CPLX>::P *__restrict__ psi, Dim
    }
    rowA[row] = a.finish(hz);
    if (rowB) rowB[row] = b.finish(hz);
-}
-
-// Weight of sample k in simpint over N samples (src/utils/diffint.cu:37-66),
-// in units of h/3: 1, 4, 2, ..., 4, 1 over the first odd count of samples,
-// plus the end correction (5 f[N-1] + 8 f[N-2] - f[N-3]) / 4 for even N.
-__device__ __forceinline__ double simp_w(int k, int N) {
-   const int mm = (N & 1) ? N : N - 1;
-   double w = k < mm ? ((k == 0 || k == mm - 1) ? 1. : ((k & 1) ? 4. : 2.)) : 0.;
-   if (!(N & 1)) {
-      if (k == N - 1) w += 1.25;
-      else if (k == N - 2) w += 2.;
-      else if (k == N - 3) w -= 0.25;
-   }
-   return w;
 }
 
 // norm = sqrt(S_x S_y rowsum) (calcnorm, imag3d-mpicuda.cu:1194-1218), stores

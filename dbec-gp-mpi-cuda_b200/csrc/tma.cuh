@@ -84,13 +84,17 @@ __device__ __forceinline__ bool consumer_any(bool flag, int nthreads) {
    return r != 0;
 }
 
-// Bounded wait for phase `parity` of `bar`.  Returns false (and sets bit
-// kErrTmaTimeout in *err) when the copy did not complete in time.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t *err) {
-   for (uint32_t i = 0; i < kMaxSpins; i++)
+// Bounded wait for phase `parity` of `bar`: at most `spins` polls.  Returns
+// false (and sets bit kErrTmaTimeout in *err) when the phase did not complete
+// in time.
+__device__ __forceinline__ bool mbar_wait_n(uint64_t *bar, uint32_t parity, uint32_t *err, uint32_t spins) {
+   for (uint32_t i = 0; i < spins; i++)
       if (mbar_try_wait(bar, parity)) return true;
    if (err) atomicOr(err, kErrTmaTimeout);
    return false;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t *err) {
+   return mbar_wait_n(bar, parity, err, kMaxSpins);
 }
 
 // 3D tiled tensor load global -> shared, completing on bar.

@@ -20,7 +20,8 @@ PREC_FP64, PREC_MIXED = 0, 1
 DENSITY = {"1d_x": 0, "1d_y": 1, "1d_z": 2, "2d_xy": 3, "2d_xz": 4, "2d_yz": 5,
            "3d_xy0": 6, "3d_x0z": 7, "3d_0yz": 8, "3d": 9}
 STATUS = {0: "GPE_OK", 1: "GPE_ERR_PARAM", 2: "GPE_ERR_CUDA", 3: "GPE_ERR_OOM", 4: "GPE_ERR_TIMEOUT",
-          5: "GPE_ERR_STATE", 6: "GPE_ERR_IO", 7: "GPE_ERR_UNSUPPORTED", 8: "GPE_ERR_BUDGET"}
+          5: "GPE_ERR_STATE", 6: "GPE_ERR_IO", 7: "GPE_ERR_UNSUPPORTED", 8: "GPE_ERR_BUDGET",
+          9: "GPE_ERR_CANCELLED"}
 
 
 class GpeError(RuntimeError):
@@ -86,8 +87,10 @@ _SIGS = {
     "gpe_calcluy": (C.c_int, [_P]),
     "gpe_calcluz": (C.c_int, [_P]),
     "gpe_synchronize": (C.c_int, [_P]),
+    "gpe_selftest_wait_timeout": (C.c_int, [_P, C.c_uint]),
     "gpe_launch_count": (C.c_int, [_P, C.POINTER(C.c_longlong)]),
     "gpe_time_steps": (C.c_int, [_P, C.c_long, _D, _D, _DP]),
+    "gpe_time_calcpsidd2": (C.c_int, [_P, C.c_long, _DP]),
     "gpe_profile_step": (C.c_int, [_P, C.c_long, _D, _D, _P, C.c_int, C.POINTER(C.c_int)]),
     "gpe_step_kernel_name": (C.c_char_p, [_P, C.c_int]),
     "gpe_step_kernel_bytes": (C.c_double, [_P, C.c_int]),
@@ -109,6 +112,7 @@ _SIGS = {
     "gpe_server_destroy": (None, [_P]),
     "gpe_server_submit": (C.c_int, [_P, C.POINTER(Request), C.POINTER(C.c_longlong)]),
     "gpe_server_wait": (C.c_int, [_P, C.c_longlong, _D, C.POINTER(Result)]),
+    "gpe_server_cancel": (C.c_int, [_P, C.c_longlong]),
     "gpe_server_stats": (C.c_int, [_P, _DP]),
 }
 
@@ -154,6 +158,41 @@ def norm_noalloc(psi_dev_ptr, mode, nx, ny, nz, dx, dy, dz, norm_dev_ptr, stream
     _check(lib().gpe_norm_noalloc(C.c_void_p(psi_dev_ptr), int(mode), int(nx), int(ny), int(nz), float(dx),
                                   float(dy), float(dz), C.c_void_p(norm_dev_ptr),
                                   C.c_void_p(stream) if stream else None))
+
+
+CUFFT_LIB_PATH = os.path.join(_PKG, "lib", "libgpe_cufft.so")
+_cufft = None
+
+
+def cufft_lib():
+    """The cuFFT comparison library (libgpe_cufft.so, include/gpe_cufft.h)."""
+    global _cufft
+    if _cufft is None:
+        if not os.path.exists(CUFFT_LIB_PATH):
+            raise OSError("libgpe_cufft.so not built: run dbec-gp-mpi-cuda_b200/build.py (%s)" % CUFFT_LIB_PATH)
+        L = C.CDLL(CUFFT_LIB_PATH)
+        L.gpe_cufft_convolution.restype = C.c_int
+        L.gpe_cufft_convolution.argtypes = [C.POINTER(Params), _P, C.c_int, C.c_int, _P, _DP]
+        L.gpe_cufft_last_error.restype = C.c_char_p
+        L.gpe_cufft_last_error.argtypes = []
+        _cufft = L
+    return _cufft
+
+
+def cufft_convolution(params: Params, psi, variant=1, nrep=5):
+    """phi and the mean milliseconds per convolution of the cuFFT pipeline
+    (variant 0: the reference's call structure; 1: batched x transforms)."""
+    L = cufft_lib()
+    if params.mode == MODE_IMAG:
+        buf = np.ascontiguousarray(np.asarray(psi).real, dtype=np.float64)
+    else:
+        buf = np.ascontiguousarray(psi, dtype=np.complex128)
+    phi = np.empty((params.nx, params.ny, params.nz))
+    ms = C.c_double()
+    st = L.gpe_cufft_convolution(C.byref(params), _ptr(buf), int(variant), int(nrep), _ptr(phi), C.byref(ms))
+    if st != 0:
+        raise GpeError(st, L.gpe_cufft_last_error().decode())
+    return phi, ms.value
 
 
 def device_bytes(params: Params) -> int:
@@ -280,10 +319,20 @@ class Solver:
     def synchronize(self):
         _check(lib().gpe_synchronize(self.h))
 
+    def selftest_wait_timeout(self, spins=4096):
+        """Queues a bounded wait that nothing completes (see gpe.h)."""
+        _check(lib().gpe_selftest_wait_timeout(self.h, int(spins)))
+
     def launch_count(self):
         v = C.c_longlong()
         _check(lib().gpe_launch_count(self.h, C.byref(v)))
         return v.value
+
+    def time_calcpsidd2(self, nrep):
+        """Mean milliseconds of one dipolar convolution (nrep timed calls)."""
+        ms = C.c_double()
+        _check(lib().gpe_time_calcpsidd2(self.h, int(nrep), C.byref(ms)))
+        return ms.value
 
     def profile_step(self, nsteps, g, gd):
         """Mean per-kernel duration (ms) over nsteps steps: [(name, ms, bytes)]."""
@@ -406,6 +455,9 @@ class Server:
         r = Result()
         _check(lib().gpe_server_wait(self.h, int(rid), float(timeout), C.byref(r)))
         return r
+
+    def cancel(self, rid):
+        _check(lib().gpe_server_cancel(self.h, int(rid)))
 
     def stats(self):
         v = (C.c_double * 4)()

@@ -36,7 +36,8 @@ typedef enum {
    GPE_ERR_STATE = 5,       /* call not valid in the handle's state */
    GPE_ERR_IO = 6,          /* file could not be read or written */
    GPE_ERR_UNSUPPORTED = 7, /* feature not available in this build */
-   GPE_ERR_BUDGET = 8       /* admission refused by the memory budget */
+   GPE_ERR_BUDGET = 8,      /* admission refused by the memory budget */
+   GPE_ERR_CANCELLED = 9    /* request cancelled (gpe_server_cancel) */
 } gpe_status;
 
 enum { GPE_MODE_IMAG = 0, GPE_MODE_REAL = 1 };
@@ -121,11 +122,24 @@ gpe_status gpe_calcluy(gpe_solver *s);                  /* calcluy, imag3d:1851-
 gpe_status gpe_calcluz(gpe_solver *s);                  /* calcluz, imag3d:1907-1942 */
 gpe_status gpe_synchronize(gpe_solver *s);
 
+/* Self-test of the bounded device waits (no reference counterpart: the
+ * reference's kernels never wait on the device).  Queues one CTA that waits,
+ * polling at most `spins` times (1..65536), on an mbarrier expecting a
+ * transaction that no copy delivers; no copy is issued, so nothing is in
+ * flight when it gives up.  The next gpe_synchronize (or gpe_run) returns
+ * GPE_ERR_TIMEOUT and clears the handle's status word, after which the handle
+ * works normally. */
+gpe_status gpe_selftest_wait_timeout(gpe_solver *s, unsigned spins);
 /* Kernel launches queued by this handle since creation (for accounting). */
 gpe_status gpe_launch_count(gpe_solver *s, long long *count);
 /* Step timing on the handle's stream: runs nsteps plain steps (fixed g, gd)
  * bracketed by CUDA events and returns the elapsed milliseconds. */
 gpe_status gpe_time_steps(gpe_solver *s, long nsteps, double g, double gd, double *ms);
+/* Timing of the dipolar convolution alone (calcpsidd2, imag3d-mpicuda.cu:
+ * 1460-1510): after one untimed call, nrep calls bracketed by CUDA events on
+ * the handle's stream; *ms receives the mean milliseconds per call (the
+ * figure gpe_cufft_convolution in gpe_cufft.h is compared with). */
+gpe_status gpe_time_calcpsidd2(gpe_solver *s, long nrep, double *ms);
 /* Per-kernel timing: runs nsteps plain steps with a CUDA event around every
  * kernel of the step and returns, per kernel of one step, the mean duration in
  * milliseconds (ms[i], i < *count <= cap).  gpe_step_kernel_name(i) names
@@ -230,6 +244,12 @@ gpe_status gpe_server_submit(gpe_server *sv, const gpe_request *rq, long long *i
 /* Waits (at most timeout_s seconds, < 0 = forever) for request id; fills res.
  * GPE_ERR_TIMEOUT when it has not finished in time. */
 gpe_status gpe_server_wait(gpe_server *sv, long long id, double timeout_s, gpe_result *res);
+/* Cancels request id.  A queued request is finished at once; an admitted one
+ * stops at its next chunk boundary (no kernels of it in flight), its memory
+ * is freed, and its result (gpe_server_wait) has status GPE_ERR_CANCELLED and
+ * the steps it ran.  GPE_ERR_STATE when the request has already finished,
+ * GPE_ERR_PARAM for an unknown id. */
+gpe_status gpe_server_cancel(gpe_server *sv, long long id);
 /* stats[0] requests done, [1] peak active, [2] peak bytes admitted, [3] chunks run. */
 gpe_status gpe_server_stats(gpe_server *sv, double *stats);
 
@@ -237,14 +257,18 @@ gpe_status gpe_server_stats(gpe_server *sv, double *stats);
  * the reference: it serves callers that cannot call cudaMalloc where they need
  * the norm (a latency-critical loop that must not take cudaMalloc/cudaFree's
  * implicit synchronisation, or a process whose device memory belongs to
- * another allocator).  psi_dev: nx*ny*nz doubles (mode GPE_MODE_IMAG) or
- * interleaved complex doubles (GPE_MODE_REAL), x-major; norm_dev: one device
- * double that receives sqrt(Simpson integral of |psi|^2), as calcnorm.  Work
- * is queued on stream (NULL = default stream) and nothing is allocated: the
- * per-row partials live in a 2 MiB file-scope device array, so nx*ny must be
- * at most 262144 and nx at most 1024 (GPE_ERR_PARAM otherwise).  The first
- * call on a device looks up that array's address; make it before any stream
- * capture.  Calls that overlap on the GPU share the array and race. */
+ * another allocator).  psi_dev: nx*ny*nz doubles (mode GPE_MODE_IMAG, 8-byte
+ * aligned) or interleaved complex doubles (GPE_MODE_REAL, 16-byte aligned),
+ * x-major; norm_dev: one 8-byte aligned device double that receives
+ * sqrt(Simpson integral of |psi|^2), as calcnorm.  Work is queued on stream
+ * (NULL = default stream) and nothing is allocated: the per-row partials live
+ * in a 2 MiB file-scope device array, so nx*ny must be at most 262144 and nx,
+ * nz at most 1024; sizes beyond that and misaligned pointers are refused with
+ * GPE_ERR_PARAM before anything is launched.  The first call in a CUDA context
+ * looks up that array's address and caches it for the context (a context
+ * created after cudaDeviceReset looks it up again); make that first call
+ * before any stream capture.  Calls that overlap on the GPU share the array
+ * and race. */
 gpe_status gpe_norm_noalloc(const void *psi_dev, int mode, long nx, long ny, long nz, double dx, double dy, double dz,
                             double *norm_dev, void *stream);
 

@@ -1,6 +1,9 @@
 """Copies the reference's shipped golden outputs and sample inputs into this
-directory as test fixtures (run once, in a checkout that has the reference
-next to it; the fixtures are committed, so tests never read the reference).
+directory as test fixtures (run once, with the path of a checkout of the
+reference as the only argument; the fixtures are committed, so tests never
+read the reference).
+
+Usage: python tests/golden/make_golden.py <reference project root>
 
 Sources, relative to the reference project root:
   input/imag3d-input, input/real3d-input            parameter files
@@ -13,7 +16,6 @@ import os
 import shutil
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 FILES = [
@@ -28,6 +30,9 @@ FILES = [
   + [("output/real3d-mpicuda/real3d-den1d_%s.bin" % a, "real3d-den1d_%s.bin" % a) for a in "xyz"]
 
 if __name__ == "__main__":
+    if len(sys.argv) != 2:
+        sys.exit("usage: python make_golden.py <reference project root>")
+    REF = sys.argv[1]
     for src, dst in FILES:
         shutil.copyfile(os.path.join(REF, src), os.path.join(HERE, dst))
         print(dst)

@@ -6,6 +6,7 @@ import os
 import re
 import subprocess
 
+import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -157,3 +158,26 @@ def test_server_rejects_bad_requests_on_the_host(gpe_lib):
             sv.submit(p, kind, 1., 0., **kw)
         assert e.value.status == 1
     sv.close()
+
+
+def test_server_cancel_unknown_id_on_the_host(gpe_lib):
+    gpe = gpe_lib
+    sv = gpe.Server(1 << 30, device=0)
+    with pytest.raises(gpe.GpeError) as e:
+        sv.cancel(12345)
+    assert e.value.status == 1
+    sv.close()
+
+
+def test_cufft_library_exports_its_declared_symbols(gpe_lib):
+    txt = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "gpe_cufft.h")).read(), flags=re.S)
+    names = sorted(set(re.findall(r"\b(gpe_[a-z0-9_]+)\s*\(", txt)))
+    assert names == ["gpe_cufft_convolution", "gpe_cufft_last_error"]
+    L = gpe_lib.cufft_lib()
+    for n in names:
+        assert hasattr(L, n)
+    # argument checks run before any CUDA call
+    p = gpe_lib.make_params(0, 15, 16, 16, .2, .2, .2, .004, 1., 1., 1., 1.6)
+    with pytest.raises(gpe_lib.GpeError) as e:
+        gpe_lib.cufft_convolution(p, np.zeros((15, 16, 16)))
+    assert e.value.status == 1

@@ -122,3 +122,32 @@ def test_mixed_real_time(gpe_lib, oracle_mod):
     _observables_close(s, o, 50., 20., RT_ENERGY_TOL, RT_SIZE_TOL)
     assert dens_l2(s.get_psi(), o.get_psi()) <= RT_DENS_TOL
     s.close()
+
+
+def test_mixed_512x512x256_against_fp64_gpu(gpe_lib):
+    """The mixed-precision configuration at its own size: imaginary time at
+    512x512x256, dx = 0.25, dt = 0.1 dx^2, trap (0.5, 1, 1.5), g = 100,
+    gd = 30, R = 32, the reference Gaussian start, 500 renormalised steps.
+    The stand-in oracle at this size is the plain FP64 GPU path, which the
+    64^3 and 256^3 tests pin to the oracle at 1e-10.  Bars: |dmu/mu|, |dE/E|,
+    rms sizes and the last pre-renormalisation norm <= 1e-6 relative, density
+    L2 <= 1e-5 (the mixed path's stated accuracy)."""
+    gpe = gpe_lib
+    shape, h, dt, trap = (512, 512, 256), .25, .00625, (.5, 1., 1.5)
+    g, gd, nsteps = 100., 30., 500
+    out = {}
+    for prec in (gpe.PREC_FP64, gpe.PREC_MIXED):
+        s = gpe.Solver(gpe.make_params(0, *shape, h, h, h, dt, *trap, 32.0, precision=prec))
+        s.init_gaussian()
+        s.calcnorm(True)
+        _, _, last_norm, _ = s.run(nsteps, g, gd)
+        mu, en = s.calcmuen(g, gd)
+        out[prec] = dict(mu=mu, en=en, rms=s.calcrms(), norm=last_norm, psi=s.get_psi())
+        s.close()
+    a, b = out[gpe.PREC_MIXED], out[gpe.PREC_FP64]
+    errs = dict(mu=abs(a["mu"] / b["mu"] - 1), en=abs(a["en"] / b["en"] - 1), rms=rel(a["rms"], b["rms"]),
+                norm=abs(a["norm"] / b["norm"] - 1), dens_l2=dens_l2(a["psi"], b["psi"]))
+    print("mixed 512x512x256, %d steps, errors against the FP64 GPU path: %s" % (nsteps, errs))
+    for k in ("mu", "en", "rms", "norm"):
+        assert errs[k] <= MIX_OBS_TOL, errs
+    assert errs["dens_l2"] <= MIX_DENS_TOL, errs

@@ -236,3 +236,63 @@ def test_operators_edge_shapes(gpe_lib, oracle_mod, mode, shape):
         assert abs(rs[2] / ro[2] - 1) <= OP_TOL
     assert rel(s.calcrms(), o.calcrms()) <= OP_TOL
     s.close()
+
+
+# ---- the configurations the benchmark times, at full size -------------------
+# 256^3 real time is the bench's `real256` workload (dx = 0.2, dt = 0.01 dx^2,
+# trap (1, 1, 4), g = 200, gd = 60 quenched to 80, R = 25.6); 256^3 imaginary
+# time is the ground-state half of the same configuration (dt = 0.1 dx^2,
+# gd = 60).  Three steps of each through the C ABI against the oracle's three
+# steps, every observable and psi within the plain FP64 path's 1e-10.
+C2 = dict(shape=(256, 256, 256), spacing=(.2, .2, .2), trap=(1., 1., 4.), cutoff=25.6)
+
+
+def test_real256_bench_workload_matches_oracle(gpe_lib, oracle_mod):
+    s, o = make_pair(gpe_lib, oracle_mod, 1, C2["shape"], spacing=C2["spacing"], dt=0.01 * 0.2 * 0.2,
+                     trap=C2["trap"], cutoff=C2["cutoff"])
+    s.init_gaussian()
+    o.init_gaussian()
+    g, gd = 200., 80.
+    rs = s.run(3, g, gd, rms_every=1)
+    trace = []
+    for _ in range(3):
+        o.run(1, g, gd)
+        trace.append(o.calcrms())
+    assert rel(rs[3], np.array(trace)) <= RUN_TOL
+    _compare_observables(s, o, g, gd, RUN_TOL)
+    assert rel(s.get_psi(), o.get_psi()) <= RUN_TOL
+    s.close()
+    o.close()
+
+
+def test_imag256_matches_oracle(gpe_lib, oracle_mod):
+    s, o = make_pair(gpe_lib, oracle_mod, 0, C2["shape"], spacing=C2["spacing"], dt=0.1 * 0.2 * 0.2,
+                     trap=C2["trap"], cutoff=C2["cutoff"])
+    s.init_gaussian()
+    o.init_gaussian()
+    assert abs(s.calcnorm(True) / o.calcnorm(True) - 1) <= OP_TOL
+    rs, ro = _run_both(s, o, 3, 200., 60.)
+    assert abs(rs[2] / ro[2] - 1) <= RUN_TOL
+    _compare_observables(s, o, 200., 60., RUN_TOL)
+    assert rel(s.get_psi(), o.get_psi()) <= RUN_TOL
+    s.close()
+    o.close()
+
+
+def test_rms_trace_longer_than_device_slots(gpe_lib, oracle_mod):
+    """gpe_run keeps 256 rms samples on the device and copies every full batch
+    out while it continues: 300 samples cross that boundary."""
+    shape = (16, 12, 10)
+    s, o = make_pair(gpe_lib, oracle_mod, 1, shape, dt=.0005)
+    psi = seeded_psi(shape, 1, seed=13)
+    s.set_psi(psi)
+    o.set_psi(psi)
+    rs = s.run(600, 40., 10., rms_every=2)
+    trace = []
+    for c in range(600):
+        o.run(1, 40., 10.)
+        if c % 2 == 0:
+            trace.append(o.calcrms())
+    assert rs[3].shape == (300, 4)
+    assert rel(rs[3], np.array(trace)) <= RUN_TOL
+    s.close()
