@@ -80,12 +80,12 @@ __device__ __forceinline__ void zfwd_split(const cpx<R> *Z, const cpx<R> *tw, in
 // Pass 1: |psi|^2 rows -> half spectrum rows (L rows per CTA).
 // Register budget: four CTAs per SM for 8-row tiles, three for 16-row tiles
 // (whose shared tiles allow no more; measured faster with the larger budget).
+// The pass over the tile of L rows starting at row r0 (shared by the single
+// solve's kernel and the batched one).
 template <class R, bool CPLX, int PPT, int L>
-__global__ void __launch_bounds__(256, L >= 16 ? 3 : 4) k_zfwd(const typename Tr<R, CPLX>::P *__restrict__ psi,
-                                              cpx<R> *__restrict__ spec, Dims d, FftPlan ph,
-                                              const cpx<R> *__restrict__ twz, int LSr, uint32_t *err) {
-   pdl_trigger();
-   pdl_wait();
+__device__ __forceinline__ void zfwd_body(const typename Tr<R, CPLX>::P *__restrict__ psi, cpx<R> *__restrict__ spec,
+                                          const Dims &d, const FftPlan &ph, const cpx<R> *__restrict__ twz, int LSr,
+                                          uint32_t *err, long long r0) {
    using C = cpx<R>;
    using P = typename Tr<R, CPLX>::P;
 
@@ -96,7 +96,6 @@ __global__ void __launch_bounds__(256, L >= 16 ? 3 : 4) k_zfwd(const typename Tr
    P *rows = (P *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
    C *buf = (C *) (rows + L * LSr);
    C *tw = buf + h * L;
-   const long long r0 = (long long) blockIdx.x * L;
    const int nr = (int) ((d.nxy - r0) < L ? (d.nxy - r0) : L);
    const uint32_t row_bytes = (uint32_t) (nz * sizeof(P));
    if (threadIdx.x == 0) {
@@ -125,15 +124,23 @@ __global__ void __launch_bounds__(256, L >= 16 ? 3 : 4) k_zfwd(const typename Tr
    }
 }
 
+template <class R, bool CPLX, int PPT, int L>
+__global__ void __launch_bounds__(256, L >= 16 ? 3 : 4) k_zfwd(const typename Tr<R, CPLX>::P *__restrict__ psi,
+                                              cpx<R> *__restrict__ spec, Dims d, FftPlan ph,
+                                              const cpx<R> *__restrict__ twz, int LSr, uint32_t *err) {
+   pdl_trigger();
+   pdl_wait();
+   zfwd_body<R, CPLX, PPT, L>(psi, spec, d, ph, twz, LSr, err, (long long) blockIdx.x * L);
+}
+
 // Passes 2 and 4: FFT along y of L kz columns of one x plane.  The host sizes
 // the CTA at one thread per PPT points of the tile (128 threads for the
 // 4-column FP64 tiles, so that eight fit on an SM); the register budget
 // (launch bounds 256 x 4) allows any of these sizes.
 template <class R, bool INV, int L>
-__global__ void __launch_bounds__(256, 4) k_yfft(const __grid_constant__ CUtensorMap tm, Dims d, FftPlan py,
-                                                 const cpx<R> *__restrict__ twy, int boxn, int nbox, uint32_t *err) {
-   pdl_trigger();
-   pdl_wait();
+__device__ __forceinline__ void yfft_body(const CUtensorMap *tm, const Dims &d, const FftPlan &py,
+                                          const cpx<R> *__restrict__ twy, int boxn, int nbox, uint32_t *err, int x,
+                                          int k0) {
    using C = cpx<R>;
    constexpr int PPT = FftL<R>::PPT;
    extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -141,8 +148,6 @@ __global__ void __launch_bounds__(256, 4) k_yfft(const __grid_constant__ CUtenso
    const int ny = d.ny, rows = boxn * nbox;
    C *buf = (C *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
    C *tw = buf + rows * L;
-   const int nkb = (d.nzh + L - 1) / L;
-   const int x = blockIdx.x / nkb, k0 = (blockIdx.x - x * nkb) * L;
    if (threadIdx.x == 0) {
       mbar_init(&bar, 1);
       fence_mbar_init();
@@ -151,28 +156,37 @@ __global__ void __launch_bounds__(256, 4) k_yfft(const __grid_constant__ CUtenso
    if (threadIdx.x == 0) {
       mbar_arrive_expect_tx(&bar, (uint32_t) (rows * L * sizeof(C) + ny * sizeof(C)));
       bulk_load(tw, twy, (uint32_t) (ny * sizeof(C)), &bar);
-      for (int b = 0; b < nbox; b++) tma_load_3d(buf + b * boxn * L, &tm, 2 * k0, b * boxn, x, &bar);
+      for (int b = 0; b < nbox; b++) tma_load_3d(buf + b * boxn * L, tm, 2 * k0, b * boxn, x, &bar);
    }
    if (__syncthreads_or(!mbar_wait(&bar, 0, err))) return;
    fft_lines_ip<L, C, INV, PPT>(buf, py, tw, 1);
    fence_proxy_async();
    __syncthreads();
    if (threadIdx.x == 0) {
-      for (int b = 0; b < nbox; b++) tma_store_3d(&tm, 2 * k0, b * boxn, x, buf + b * boxn * L);
+      for (int b = 0; b < nbox; b++) tma_store_3d(tm, 2 * k0, b * boxn, x, buf + b * boxn * L);
       bulk_commit();
       bulk_wait_all();
    }
+}
+
+template <class R, bool INV, int L>
+__global__ void __launch_bounds__(256, 4) k_yfft(const __grid_constant__ CUtensorMap tm, Dims d, FftPlan py,
+                                                 const cpx<R> *__restrict__ twy, int boxn, int nbox, uint32_t *err) {
+   pdl_trigger();
+   pdl_wait();
+   const int nkb = (d.nzh + L - 1) / L;
+   const int x = blockIdx.x / nkb, k0 = (blockIdx.x - x * nkb) * L;
+   yfft_body<R, INV, L>(&tm, d, py, twy, boxn, nbox, err, x, k0);
 }
 
 // Pass 3: FFT along x, multiply by Udd(k) * scale^2, inverse FFT along x, for
 // L kz columns of one y plane.  Udd octant layout [|kx|][|ky|][kz].  CTA size
 // as for the y passes.
 template <class R, int L>
-__global__ void __launch_bounds__(256, 4) k_xconv(const __grid_constant__ CUtensorMap tm, Dims d, FftPlan px,
-                                                  const cpx<R> *__restrict__ twx, const double *__restrict__ udd,
-                                                  const State *__restrict__ st, int boxn, int nbox, uint32_t *err) {
-   pdl_trigger();
-   pdl_wait();
+__device__ __forceinline__ void xconv_body(const CUtensorMap *tm, const Dims &d, const FftPlan &px,
+                                           const cpx<R> *__restrict__ twx, const double *__restrict__ udd,
+                                           const State *__restrict__ st, int boxn, int nbox, uint32_t *err, int y,
+                                           int k0) {
    using C = cpx<R>;
    constexpr int PPT = FftL<R>::PPT;
    extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -181,8 +195,6 @@ __global__ void __launch_bounds__(256, 4) k_xconv(const __grid_constant__ CUtens
    C *buf = (C *) (((uintptr_t) smem_raw + 127) & ~(uintptr_t) 127);
    C *tw = buf + rows * L;
    double *ud = (double *) (tw + nx);  // Udd of this y plane and these columns, [|kx|][L]
-   const int nkb = (d.nzh + L - 1) / L;
-   const int y = blockIdx.x / nkb, k0 = (blockIdx.x - y * nkb) * L;
    const int nxh = nx / 2 + 1, nyh = ny / 2 + 1, nzh = d.nzh;
    const int ay = (y <= ny / 2) ? y : ny - y;
    if (threadIdx.x == 0) {
@@ -193,7 +205,7 @@ __global__ void __launch_bounds__(256, 4) k_xconv(const __grid_constant__ CUtens
    if (threadIdx.x == 0) {
       mbar_arrive_expect_tx(&bar, (uint32_t) (rows * L * sizeof(C) + nx * sizeof(C)));
       bulk_load(tw, twx, (uint32_t) (nx * sizeof(C)), &bar);
-      for (int b = 0; b < nbox; b++) tma_load_3d(buf + b * boxn * L, &tm, 2 * k0, y, b * boxn, &bar);
+      for (int b = 0; b < nbox; b++) tma_load_3d(buf + b * boxn * L, tm, 2 * k0, y, b * boxn, &bar);
    }
    // the Udd factors of the tile travel while the tile and the forward FFT do
    // (loaded after the FFT, their latency measured exposed)
@@ -222,18 +234,28 @@ __global__ void __launch_bounds__(256, 4) k_xconv(const __grid_constant__ CUtens
    fence_proxy_async();
    __syncthreads();
    if (threadIdx.x == 0) {
-      for (int b = 0; b < nbox; b++) tma_store_3d(&tm, 2 * k0, y, b * boxn, buf + b * boxn * L);
+      for (int b = 0; b < nbox; b++) tma_store_3d(tm, 2 * k0, y, b * boxn, buf + b * boxn * L);
       bulk_commit();
       bulk_wait_all();
    }
 }
 
-// Pass 5: half spectrum rows -> phi rows (unnormalised inverse, Hermitian).
-template <class R, int PPT, int L>
-__global__ void __launch_bounds__(256, L >= 16 ? 3 : 4) k_zinv(const cpx<R> *__restrict__ spec, R *__restrict__ phi, Dims d,
-                                                 FftPlan ph, const cpx<R> *__restrict__ twz, int LSo, uint32_t *err) {
+template <class R, int L>
+__global__ void __launch_bounds__(256, 4) k_xconv(const __grid_constant__ CUtensorMap tm, Dims d, FftPlan px,
+                                                  const cpx<R> *__restrict__ twx, const double *__restrict__ udd,
+                                                  const State *__restrict__ st, int boxn, int nbox, uint32_t *err) {
    pdl_trigger();
    pdl_wait();
+   const int nkb = (d.nzh + L - 1) / L;
+   const int y = blockIdx.x / nkb, k0 = (blockIdx.x - y * nkb) * L;
+   xconv_body<R, L>(&tm, d, px, twx, udd, st, boxn, nbox, err, y, k0);
+}
+
+// Pass 5: half spectrum rows -> phi rows (unnormalised inverse, Hermitian).
+template <class R, int PPT, int L>
+__device__ __forceinline__ void zinv_body(const cpx<R> *__restrict__ spec, R *__restrict__ phi, const Dims &d,
+                                          const FftPlan &ph, const cpx<R> *__restrict__ twz, int LSo, uint32_t *err,
+                                          long long r0) {
    using C = cpx<R>;
 
    extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -244,7 +266,6 @@ __global__ void __launch_bounds__(256, L >= 16 ? 3 : 4) k_zinv(const cpx<R> *__r
    const int in_elems = ((L * nzp) > (L * LSo + 1) / 2 ? (L * nzp) : (L * LSo + 1) / 2);
    C *buf = in + ((in_elems + 7) & ~7);
    C *tw = buf + h * L;
-   const long long r0 = (long long) blockIdx.x * L;
    const int nr = (int) ((d.nxy - r0) < L ? (d.nxy - r0) : L);
    if (threadIdx.x == 0) {
       mbar_init(&bar, 1);
@@ -295,6 +316,14 @@ __global__ void __launch_bounds__(256, L >= 16 ? 3 : 4) k_zinv(const cpx<R> *__r
    }
 }
 
+template <class R, int PPT, int L>
+__global__ void __launch_bounds__(256, L >= 16 ? 3 : 4) k_zinv(const cpx<R> *__restrict__ spec, R *__restrict__ phi, Dims d,
+                                                 FftPlan ph, const cpx<R> *__restrict__ twz, int LSo, uint32_t *err) {
+   pdl_trigger();
+   pdl_wait();
+   zinv_body<R, PPT, L>(spec, phi, d, ph, twz, LSo, err, (long long) blockIdx.x * L);
+}
+
 // Boundary planes of phi at one rank (calcpsidd2_kernel2a/2b with last = 1,
 // imag3d-mpicuda.cu:1591-1625): x = nx-1 <- x = 0 and y = ny-1 <- y = 0 here,
 // each excluding the other two last indices; z = nz-1 <- z = 0 is done inside
@@ -303,10 +332,7 @@ __global__ void __launch_bounds__(256, L >= 16 ? 3 : 4) k_zinv(const cpx<R> *__r
 // j) <- (0, j), blocks [ny-1, ny-1 + nx-1) the rows (i, ny-1) <- (i, 0), the
 // first nz-1 points of each (the grid has at least one block).
 template <class R>
-__global__ void k_phifix(R *__restrict__ phi, Dims d) {
-   pdl_trigger();
-   pdl_wait();
-   const int b = blockIdx.x;
+__device__ __forceinline__ void phifix_body(R *__restrict__ phi, const Dims &d, int b) {
    long long dst, src;
    if (b < d.ny - 1) {
       dst = ((long long) (d.nx - 1) * d.ny + b) * d.nz;
@@ -319,6 +345,13 @@ __global__ void k_phifix(R *__restrict__ phi, Dims d) {
       return;
    }
    for (int k = threadIdx.x; k < d.nz - 1; k += blockDim.x) phi[dst + k] = phi[src + k];
+}
+
+template <class R>
+__global__ void k_phifix(R *__restrict__ phi, Dims d) {
+   pdl_trigger();
+   pdl_wait();
+   phifix_body<R>(phi, d, blockIdx.x);
 }
 
 // Self-test of the bounded waits: one CTA waits on an mbarrier that expects
@@ -384,13 +417,11 @@ __global__ void k_rows_dens(const typename Tr<R, CPLX>::P *__restrict__ psi, Dim
 // (a few kB of row sums): loads are issued ahead of the sums and the final
 // sum uses the whole CTA (16 -> 10 us at 256^3).
 constexpr int kNormRowsPerCta = 8;
-__global__ void __launch_bounds__(32 * kNormRowsPerCta) k_norm_final(const double *__restrict__ rowsum, Dims d,
-                                                                     double hx, double hy, State *st, double *xs,
-                                                                     double *out_norm) {
-   pdl_trigger();
-   pdl_wait();
+// CTA `cta` of the `ncta` CTAs that reduce one solve's row sums.
+__device__ __forceinline__ void norm_final_body(const double *__restrict__ rowsum, const Dims &d, double hx, double hy,
+                                                State *st, double *xs, double *out_norm, int cta, int ncta) {
    const int lane = threadIdx.x & 31;
-   const int i = blockIdx.x * kNormRowsPerCta + (threadIdx.x >> 5);
+   const int i = cta * kNormRowsPerCta + (threadIdx.x >> 5);
    if (i < d.nx) {
       // a warp per x row; the loads of a lane are issued before the sums
       const double *r = rowsum + (long long) i * d.ny;
@@ -416,7 +447,7 @@ __global__ void __launch_bounds__(32 * kNormRowsPerCta) k_norm_final(const doubl
    __syncthreads();
    __shared__ bool last;
    __shared__ double red[32 * kNormRowsPerCta];
-   if (threadIdx.x == 0) last = atomicAdd(&st->ticket, 1u) == gridDim.x - 1;
+   if (threadIdx.x == 0) last = atomicAdd(&st->ticket, 1u) == (unsigned) ncta - 1;
    __syncthreads();
    if (!last) return;
    // last CTA: every thread takes its strided share of the x rows, then a
@@ -442,6 +473,14 @@ __global__ void __launch_bounds__(32 * kNormRowsPerCta) k_norm_final(const doubl
       st->ticket = 0u;
       if (out_norm) *out_norm = nrm;
    }
+}
+
+__global__ void __launch_bounds__(32 * kNormRowsPerCta) k_norm_final(const double *__restrict__ rowsum, Dims d,
+                                                                     double hx, double hy, State *st, double *xs,
+                                                                     double *out_norm) {
+   pdl_trigger();
+   pdl_wait();
+   norm_final_body(rowsum, d, hx, hy, st, xs, out_norm, blockIdx.x, gridDim.x);
 }
 
 // psi *= scale (calcnorm_kernel, imag3d-mpicuda.cu:1220-1233).

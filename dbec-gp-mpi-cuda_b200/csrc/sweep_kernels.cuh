@@ -266,6 +266,62 @@ template <class R> struct NuTrap {
    }
 };
 
+// FP64 calcnu over a staged tile before its sweep (the x sweep's fused
+// calcnu_kernel, imag3d-mpicuda.cu:1759, real3d-mpicuda.cu:1856), one z
+// column per thread, with the pending 1/norm applied first.  Tile t of the
+// sweep covers z columns [z0, z0 + TW) of plane `other` (y for the x sweep,
+// x for the y sweep); xtab is calcnu's per-x table staged in shared memory
+// (imaginary time: exp(-dt V_x); real time: x^2).  The caller synchronises
+// the CTA afterwards.
+template <class R, bool CPLX, int AXIS>
+__device__ __forceinline__ void nu_pass_fp64(typename Tr<R, CPLX>::P *tile, const R *ptile, int n, int lg, int c,
+                                             int other, int z0, const Dims &d, const Trap &trap, const LinPhase &lin,
+                                             const double *xtab, double g, double gd, double dt, double scale) {
+   const R invN = (R) (1.0 / (double) d.npts);
+   const int k = z0 + c;
+   if (k >= d.nz) return;
+   const int step = blockDim.x >> lg;
+   if constexpr (!CPLX && AXIS == 0) {
+      // imaginary time: trap factor exp(-dt V) from the axis tables, series
+      // for the nonlinear part (measured faster than exp of the sum; in real
+      // time CUDA's sincos of the sum measured faster than the split, so real
+      // time keeps nu_op)
+      const double eyz = __ldg((const double *) lin.ey + other) * __ldg((const double *) lin.ez + k);
+      for (int ii = threadIdx.x >> lg; ii < n; ii += step) {
+         const int e = (ii << lg) + c;
+         const double lx = xtab[ii] * eyz;
+         tile[e] = nu_split(scl(tile[e], scale), (double) ptile[e], lx, g, gd, dt, (double) invN);
+      }
+   } else {
+      // Trap::v with the terms of the two fixed coordinates hoisted
+      const double tz = mrn(trap.vl2, trap.z2[k]);
+      const double to = AXIS == 0 ? mrn(trap.vn2, trap.y2[other]) : mrn(trap.vg2, trap.x2[other]);
+      const double *va = AXIS == 0 ? xtab : trap.y2;
+      const double ca = AXIS == 0 ? trap.vg2 : trap.vn2;
+#pragma unroll 2
+      for (int ii = threadIdx.x >> lg; ii < n; ii += step) {
+         const int e = (ii << lg) + c;
+         const double sv = AXIS == 0 ? arn(arn(mrn(ca, va[ii]), to), tz) : arn(arn(to, mrn(ca, va[ii])), tz);
+         const R V = (R) mrn(trap.hp, sv);
+         tile[e] = nu_op<R>(scl(tile[e], scale), ptile[e], V, (R) g, (R) gd, (R) dt, invN);
+      }
+   }
+}
+
+// FP32: calcnu applied as the sweep's recurrence reads each point (measured
+// faster than the separate pass over the tile; slower in FP64, where a
+// thread's extra evaluations for the two points above its segment cost more).
+template <class R, int AXIS>
+__device__ __forceinline__ NuTrap<R> nu_reads_fp32(const R *ptile_c, int TW, int other, int z0, int c, const Dims &d,
+                                                   const Trap &trap, double g, double gd, double dt, double scale) {
+   const R invN = (R) (1.0 / (double) d.npts);
+   const int k = min(z0 + c, d.nz - 1);  // columns past nz are zero fill, never stored
+   const double tz = mrn(trap.vl2, trap.z2[k]);
+   const double to = AXIS == 0 ? mrn(trap.vn2, trap.y2[other]) : mrn(trap.vg2, trap.x2[other]);
+   return NuTrap<R>{ptile_c, TW, AXIS == 0 ? trap.x2 : trap.y2, AXIS == 0 ? trap.vg2 : trap.vn2, to, tz, trap.hp, scale,
+                    (R) g, (R) gd, (R) dt, invN};
+}
+
 // ---------------------------------------------------------------------------
 // Persistent pipelined CTAs.  A CTA walks the tiles t = blockIdx.x,
 // blockIdx.x + gridDim.x, ... through S shared-memory stages: while it sweeps
@@ -349,7 +405,6 @@ __global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) k_sweep_xy(const 
    __syncthreads();
    if (threadIdx.x == 0 && (int) blockIdx.x < ntiles) copy_tile(blockIdx.x, 0, true);
    const double scale = NU ? st->scale : 1.;
-   const R invN = (R) (1.0 / (double) d.npts);
    const int lg = __ffs(TW) - 1;  // TW is a power of two
    const int c = threadIdx.x & (TW - 1), p = threadIdx.x >> lg;
    int i = 0;
@@ -362,56 +417,15 @@ __global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) k_sweep_xy(const 
       // a timed-out copy makes the whole CTA leave together
       if (__syncthreads_or(!mbar_wait(&full[q], (i / S) & 1, err))) break;
       P *tile = (P *) (base + q * stage_bytes);
-      if constexpr (NU && std::is_same<R, double>::value && !CPLX && AXIS == 0) {
-         // FP64 imaginary time: trap factor exp(-dt V) from the axis tables,
-         // series for the nonlinear part (measured faster than exp of the sum;
-         // in real time CUDA's sincos of the sum measured faster than the
-         // split, so real time keeps nu_op)
-         const int other = t / nzb, z0 = (t - other * nzb) * TW;
-         const R *ptile = (const R *) (tile + rows * TW);
-         const int k = z0 + c;
-         if (k < d.nz) {
-            const int step = blockDim.x >> lg;
-            const double eyz = __ldg((const double *) lin.ey + other) * __ldg((const double *) lin.ez + k);
-            for (int ii = threadIdx.x >> lg; ii < n; ii += step) {
-               const int e = (ii << lg) + c;
-               const double lx = xtab[ii] * eyz;
-               tile[e] = nu_split(scl(tile[e], scale), (double) ptile[e], lx, g, gd, dt, (double) invN);
-            }
-         }
-         __syncthreads();
-      } else if constexpr (NU && std::is_same<R, double>::value) {
-         // every thread keeps one column (blockDim.x is a multiple of TW)
-         const int other = t / nzb, z0 = (t - other * nzb) * TW;
-         const R *ptile = (const R *) (tile + rows * TW);
-         const int k = z0 + c;
-         if (k < d.nz) {
-            // Trap::v with the terms of the two fixed coordinates hoisted
-            const double tz = mrn(trap.vl2, trap.z2[k]);
-            const double to = AXIS == 0 ? mrn(trap.vn2, trap.y2[other]) : mrn(trap.vg2, trap.x2[other]);
-            const double *va = AXIS == 0 ? xtab : trap.y2;
-            const double ca = AXIS == 0 ? trap.vg2 : trap.vn2;
-            const int step = blockDim.x >> lg;
-#pragma unroll 2
-            for (int ii = threadIdx.x >> lg; ii < n; ii += step) {
-               const int e = (ii << lg) + c;
-               const double sv = AXIS == 0 ? arn(arn(mrn(ca, va[ii]), to), tz) : arn(arn(to, mrn(ca, va[ii])), tz);
-               const R V = (R) mrn(trap.hp, sv);
-               tile[e] = nu_op<R>(scl(tile[e], scale), ptile[e], V, (R) g, (R) gd, (R) dt, invN);
-            }
-         }
+      const int other = t / nzb, z0 = (t - other * nzb) * TW;
+      if constexpr (NU && std::is_same<R, double>::value) {
+         nu_pass_fp64<R, CPLX, AXIS>(tile, (const R *) (tile + rows * TW), n, lg, c, other, z0, d, trap, lin, xtab, g,
+                                     gd, dt, scale);
          __syncthreads();
       }
       if constexpr (NU && std::is_same<R, float>::value) {
-         // FP32: calcnu on the sweep's reads (measured faster than the
-         // separate pass over the tile; slower in FP64, where a thread's
-         // extra evaluations for the two points above its segment cost more)
-         const int other = t / nzb, z0 = (t - other * nzb) * TW;
-         const int k = min(z0 + c, d.nz - 1);  // columns past nz are zero fill, never stored
-         const double tz = mrn(trap.vl2, trap.z2[k]);
-         const double to = AXIS == 0 ? mrn(trap.vn2, trap.y2[other]) : mrn(trap.vg2, trap.x2[other]);
-         const NuTrap<R> xf{(const R *) (tile + rows * TW) + c, TW, AXIS == 0 ? trap.x2 : trap.y2,
-                            AXIS == 0 ? trap.vg2 : trap.vn2, to, tz, trap.hp, scale, (R) g, (R) gd, (R) dt, invN};
+         const NuTrap<R> xf = nu_reads_fp32<R, AXIS>((const R *) (tile + rows * TW) + c, TW, other, z0, c, d, trap, g,
+                                                     gd, dt, scale);
          seg_sweep<R, CPLX, MSEG, TWC>(tile, TW, 1, c, p, TW, tb, blk, nullptr, nullptr, nullptr, nullptr, xf);
       } else {
          seg_sweep<R, CPLX, MSEG, TWC>(tile, TW, 1, c, p, TW, tb, blk, nullptr, nullptr);
@@ -421,6 +435,41 @@ __global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) k_sweep_xy(const 
       if (threadIdx.x == 0) copy_tile(t, q, false);
    }
    if (threadIdx.x == 0) bulk_wait_all();
+}
+
+// The z sweep of one staged tile of TR rows (nr of them inside the grid)
+// starting at grid row row0, with the Simpson row partials of MOM >= 1; ends
+// with the tile written back in shared memory and a CTA barrier (the caller
+// then stores it).
+template <class R, bool CPLX, int MOM, int MSEG, int TWC, bool STAB>
+__device__ __forceinline__ void zsweep_tile(typename Tr<R, CPLX>::P *tile, int nr, int TR, int LS, int c, int p,
+                                            const SegTab &tbs, typename Tr<R, CPLX>::P *blk, double *part,
+                                            double *part2, const double *__restrict__ wz,
+                                            const double *__restrict__ wz2, double hz3, double *__restrict__ rowsum,
+                                            double *__restrict__ rowsum2, long long row0) {
+   using P = typename Tr<R, CPLX>::P;
+   constexpr bool SIMP = MOM >= 1;
+   if (nr < TR) {  // rows beyond the grid are zero so their sweep stays finite
+      for (int e = threadIdx.x; e < (TR - nr) * LS; e += blockDim.x) tile[nr * LS + e] = zero_of<P>();
+      __syncthreads();
+   }
+   double my = 0., my2 = 0.;
+   seg_sweep<R, CPLX, MSEG, TWC, NoXf, STAB>(tile, 1, LS, c, p, TR, tbs, blk, SIMP ? wz : nullptr, SIMP ? &my : nullptr,
+                                             MOM == 2 ? wz2 : nullptr, MOM == 2 ? &my2 : nullptr);
+   if (SIMP && p < tbs.P) part[p * TR + c] = my;
+   if (MOM == 2 && p < tbs.P) part2[p * TR + c] = my2;
+   fence_proxy_async();
+   __syncthreads();
+   if (SIMP && p == 0 && c < nr) {
+      double sum = 0.;
+      for (int pp = 0; pp < tbs.P; pp++) sum += part[pp * TR + c];
+      rowsum[row0 + c] = sum * hz3;
+      if (MOM == 2) {
+         double sum2 = 0.;
+         for (int pp = 0; pp < tbs.P; pp++) sum2 += part2[pp * TR + c];
+         rowsum2[row0 + c] = sum2 * hz3;
+      }
+   }
 }
 
 // z sweep.  Tile: TR consecutive (x, y) rows, each copied by one bulk copy to
@@ -437,7 +486,6 @@ __global__ void __launch_bounds__(256, kSweepCtas[0]) k_sweep_z(typename Tr<R, C
                                                     uint32_t *err) {
    pdl_trigger();
    pdl_wait();
-   constexpr bool SIMP = MOM >= 1;
    const int TR = TWC > 0 ? TWC : tr_arg;
    using P = typename Tr<R, CPLX>::P;
    extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -499,28 +547,8 @@ __global__ void __launch_bounds__(256, kSweepCtas[0]) k_sweep_z(typename Tr<R, C
       }
       if (__syncthreads_or(!mbar_wait(&full[q], (i / S) & 1, err))) break;
       P *tile = (P *) (base + q * stage_bytes);
-      const int nr = nrows(t);
-      if (nr < TR) {  // rows beyond the grid are zero so their sweep stays finite
-         for (int e = threadIdx.x; e < (TR - nr) * LS; e += blockDim.x) tile[nr * LS + e] = zero_of<P>();
-         __syncthreads();
-      }
-      double my = 0., my2 = 0.;
-      seg_sweep<R, CPLX, MSEG, TWC, NoXf, STAB>(tile, 1, LS, c, p, TR, tbs, blk, SIMP ? wz : nullptr, SIMP ? &my : nullptr,
-                               MOM == 2 ? wz2 : nullptr, MOM == 2 ? &my2 : nullptr);
-      if (SIMP && p < tb.P) part[p * TR + c] = my;
-      if (MOM == 2 && p < tb.P) part2[p * TR + c] = my2;
-      fence_proxy_async();
-      __syncthreads();
-      if (SIMP && p == 0 && c < nr) {
-         double sum = 0.;
-         for (int pp = 0; pp < tb.P; pp++) sum += part[pp * TR + c];
-         rowsum[(long long) t * TR + c] = sum * hz3;
-         if (MOM == 2) {
-            double sum2 = 0.;
-            for (int pp = 0; pp < tb.P; pp++) sum2 += part2[pp * TR + c];
-            rowsum2[(long long) t * TR + c] = sum2 * hz3;
-         }
-      }
+      zsweep_tile<R, CPLX, MOM, MSEG, TWC, STAB>(tile, nrows(t), TR, LS, c, p, tbs, blk, part, part2, wz, wz2, hz3,
+                                                rowsum, rowsum2, (long long) t * TR);
       if (threadIdx.x == 0) copy_tile(t, q, false);
    }
    if (threadIdx.x == 0) bulk_wait_all();
