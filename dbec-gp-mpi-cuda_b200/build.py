@@ -30,7 +30,8 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
 
 LIB_SOURCES = ["solver.cu", "noalloc.cu", "batch.cu", "server.cpp"]
 LIB_DEPS = LIB_SOURCES + ["common.cuh", "fft.cuh", "kernels.cuh", "step_kernels.cuh", "sweep_kernels.cuh", "tma.cuh",
-                          "internal.h"]
+                          "batch_kernels.cuh", "internal.h"]
+OBJ_DIR = os.path.join(PKG, "_build")
 HOST_COMMON = ["cfg.cpp", "cli.cpp"]
 PROGRAMS = {"imag3d-mpicuda": "imag3d_main.cpp", "real3d-mpicuda": "real3d_main.cpp"}
 
@@ -54,12 +55,21 @@ def _run(cmd):
 
 
 def build_lib(force=False, verbose_ptxas=False):
+    """Compiles the library's translation units in parallel (each depends on
+    every header, so a header change rebuilds them all), then links."""
+    from concurrent.futures import ThreadPoolExecutor
     os.makedirs(LIB_DIR, exist_ok=True)
+    os.makedirs(OBJ_DIR, exist_ok=True)
     deps = [os.path.join(CSRC, f) for f in LIB_DEPS] + [os.path.join(INCLUDE, "gpe.h")]
-    if force or _stale(LIB, deps):
-        extra = ["-Xptxas", "-v"] if verbose_ptxas else []
-        _run([NVCC] + NVFLAGS + extra + ["-shared", "-o", LIB] +
-             [os.path.join(CSRC, f) for f in LIB_SOURCES] + ["-lcudart", "-lpthread"])
+    if not (force or _stale(LIB, deps)):
+        return LIB
+    extra = ["-Xptxas", "-v"] if verbose_ptxas else []
+    objs = [os.path.join(OBJ_DIR, f + ".o") for f in LIB_SOURCES]
+    jobs = [[NVCC] + NVFLAGS + extra + ["-c", "-o", o, os.path.join(CSRC, f)]
+            for f, o in zip(LIB_SOURCES, objs) if force or _stale(o, deps)]
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        list(ex.map(_run, jobs))
+    _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lpthread"])
     return LIB
 
 

@@ -1,32 +1,58 @@
 // batch.cu -- many independent solves stepped together (gpe_batch_* in
 // include/gpe.h).
 //
-// Every instance is a complete solver handle with its own stream.  One batch
-// step is one split step of every instance; the step is captured once into a
-// CUDA graph (fork from a master stream, one branch per instance on its own
-// stream, join back) and that graph is relaunched for every step, so the
-// kernels of small instances, which cannot fill the GPU alone, run side by
-// side, and the per-step host cost is one graph launch.  The per-instance
-// descriptor table is the list of handles with their parameters, couplings
-// and tile configuration (gpe_batch_autotune picks the configuration per
-// distinct grid).
+// Every instance is a complete solver handle (its own device buffers, tables
+// and step state).  Instances of the same mode and precision form a group;
+// one batch step is, per group, ONE launch per pass of the split step over
+// the tiles of all its instances (batch_kernels.cuh): a per-instance
+// descriptor table in device memory (dimensions, pointers, FFT plans,
+// coefficient tables, couplings, tensor maps) and per-pass work lists of tile
+// offsets.  The step's launches are captured once into a CUDA graph and the
+// graph is relaunched for every step, so the host cost of a batch step is one
+// graph launch and the GPU sees a few wide launches instead of many narrow
+// ones.  New couplings are written into the descriptor table (the graph stays
+// valid); a new tile configuration (gpe_batch_autotune) rebuilds the tables.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <map>
 #include <string>
 #include <tuple>
 #include <vector>
 
+#include "batch_kernels.cuh"
 #include "gpe.h"
 #include "internal.h"
+
+using namespace gpe;
+
+namespace {
+
+// One group: instances of one (mode, precision), with the aggregated launch
+// geometry of its passes.
+struct Group {
+   bool cplx = false, fp32 = false;
+   std::vector<int> members;  // instance indices
+   int Ly = 0, Lx = 0;        // FFT tile widths (the narrowest of the members)
+   BatchGeom geo{};           // maxima over the members (tiles: sums)
+   std::vector<int> start;    // [kNPass][n + 1] tile offsets
+   BatchDesc *dtab = nullptr; // device descriptor table
+   int *dstart = nullptr;     // device copy of start
+   int sweep_grid[3] = {0, 0, 0};
+   size_t sweep_smem[3] = {0, 0, 0};
+};
+
+}  // namespace
 
 struct gpe_batch {
    std::vector<gpe_solver *> inst;
    std::vector<double> g, gd;
    int dev = 0;
+   int nsm = 148;
    cudaStream_t master = nullptr;
    cudaEvent_t fork = nullptr;
-   std::vector<cudaEvent_t> join;
+   std::vector<Group> groups;
+   bool tables = false;  // groups and device tables built
    cudaGraph_t graph = nullptr;
    cudaGraphExec_t exec = nullptr;
    long long kernels_per_step = 0;
@@ -45,6 +71,11 @@ gpe_status bfail(gpe_status st, const std::string &m) {
       cudaError_t e_ = (x);                                                           \
       if (e_ != cudaSuccess) return bfail(GPE_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
    } while (0)
+#define BCKS(...)                     \
+   do {                               \
+      gpe_status s_ = (__VA_ARGS__);  \
+      if (s_ != GPE_OK) return s_;    \
+   } while (0)
 
 void drop_graph(gpe_batch *b) {
    if (b->exec) cudaGraphExecDestroy(b->exec);
@@ -53,38 +84,228 @@ void drop_graph(gpe_batch *b) {
    b->graph = nullptr;
 }
 
-// Captures one batch step: master -> fork -> every instance's step on its
-// stream -> join -> master.
+void drop_tables(gpe_batch *b) {
+   drop_graph(b);
+   for (Group &G : b->groups) {
+      if (G.dtab) cudaFree(G.dtab);
+      if (G.dstart) cudaFree(G.dstart);
+   }
+   b->groups.clear();
+   b->tables = false;
+}
+
+constexpr size_t kSmemCap = 227 * 1024;
+
+// Descriptors of a group (host copy), in member order.
+gpe_status group_descs(gpe_batch *b, const Group &G, std::vector<BatchDesc> &h) {
+   h.resize(G.members.size());
+   for (size_t k = 0; k < G.members.size(); k++) {
+      const int i = G.members[k];
+      BCKS(gpe::batch_desc(b->inst[i], G.Ly, G.Lx, b->g[i], b->gd[i], &h[k]));
+   }
+   return GPE_OK;
+}
+
+// Groups, aggregated geometry, work lists and device tables.
+gpe_status build_tables(gpe_batch *b) {
+   drop_tables(b);
+   BCK(cudaSetDevice(b->dev));
+   std::map<std::pair<int, int>, int> gi;
+   for (size_t i = 0; i < b->inst.size(); i++) {
+      gpe_params p;
+      BCKS(gpe::params_of(b->inst[i], &p));
+      const auto key = std::make_pair(p.mode, p.precision);
+      auto it = gi.find(key);
+      if (it == gi.end()) {
+         Group G;
+         G.cplx = p.mode == GPE_MODE_REAL;
+         G.fp32 = p.precision == GPE_PREC_MIXED;
+         b->groups.push_back(G);
+         it = gi.emplace(key, (int) b->groups.size() - 1).first;
+      }
+      b->groups[it->second].members.push_back((int) i);
+   }
+   for (Group &G : b->groups) {
+      const int n = (int) G.members.size();
+      G.Ly = G.Lx = 1 << 30;
+      for (int i : G.members) {
+         BatchGeom own;
+         BCKS(gpe::batch_geom(b->inst[i], 0, 0, &own));
+         G.Ly = std::min(G.Ly, own.Ly);
+         G.Lx = std::min(G.Lx, own.Lx);
+      }
+      G.start.assign((size_t) kNPass * (n + 1), 0);
+      BatchGeom &A = G.geo;
+      A = BatchGeom{};
+      for (int k = 0; k < n; k++) {
+         BatchGeom g;
+         BCKS(gpe::batch_geom(b->inst[G.members[k]], G.Ly, G.Lx, &g));
+         for (int q = 0; q < kNPass; q++) {
+            G.start[(size_t) q * (n + 1) + k + 1] = G.start[(size_t) q * (n + 1) + k] + (int) g.tiles[q];
+            A.tiles[q] += g.tiles[q];
+            A.threads[q] = std::max(A.threads[q], g.threads[q]);
+            A.smem[q] = std::max(A.smem[q], g.smem[q]);
+         }
+         A.zppt = std::max(A.zppt, g.zppt);
+         for (int a = 0; a < 3; a++) {
+            A.mseg[a] = std::max(A.mseg[a], g.mseg[a]);
+            A.stage[a] = std::max(A.stage[a], g.stage[a]);
+            A.blk[a] = std::max(A.blk[a], g.blk[a]);
+            A.extra[a] = std::max(A.extra[a], g.extra[a]);
+         }
+         A.part = std::max(A.part, g.part);
+      }
+      for (long long t : A.tiles)
+         if (t > (1LL << 31) - 1) return bfail(GPE_ERR_PARAM, "batch: too many tiles in one pass");
+      // sweeps: 2-stage pipelines; as many CTAs per SM as shared memory and
+      // the kernels' register budget allow
+      for (int a = 0; a < 3; a++) {
+         size_t sm = 128 + 2 * (size_t) A.stage[a] + A.blk[a] + A.extra[a];
+         if (a == 2) sm += 2 * (size_t) A.part;
+         if (sm > kSmemCap) return bfail(GPE_ERR_PARAM, "batch: sweep tiles exceed shared memory");
+         const int cap = a == 0 ? kSweepCtas[1] : kSweepCtas[0];
+         const int ctas = std::max(1, std::min(cap, (int) (kSmemCap / sm)));
+         G.sweep_smem[a] = sm;
+         G.sweep_grid[a] = (int) std::min<long long>(A.tiles[kPXsweep + a], (long long) ctas * b->nsm);
+      }
+      std::vector<BatchDesc> h;
+      BCKS(group_descs(b, G, h));
+      BCK(cudaMalloc(&G.dtab, sizeof(BatchDesc) * h.size()));
+      BCK(cudaMalloc(&G.dstart, sizeof(int) * G.start.size()));
+      BCK(cudaMemcpyAsync(G.dtab, h.data(), sizeof(BatchDesc) * h.size(), cudaMemcpyHostToDevice, b->master));
+      BCK(cudaMemcpyAsync(G.dstart, G.start.data(), sizeof(int) * G.start.size(), cudaMemcpyHostToDevice, b->master));
+   }
+   BCK(cudaStreamSynchronize(b->master));
+   b->tables = true;
+   return GPE_OK;
+}
+
+template <class K, class... A>
+gpe_status launch(K kern, unsigned grid, unsigned block, size_t smem, cudaStream_t st, A... args) {
+   if (grid == 0) return GPE_OK;
+   if (smem > 48 * 1024)
+      BCK(cudaFuncSetAttribute((const void *) kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+   kern<<<grid, block, smem, st>>>(args...);
+   BCK(cudaGetLastError());
+   return GPE_OK;
+}
+
+// The passes of one batch step of group G, on stream st.
+template <class R, bool CPLX> struct BatchStep {
+   using C = cpx<R>;
+   template <class F> static gpe_status with_ppt(int ppt, F f) {
+      if (ppt <= 8) return f(std::integral_constant<int, 8>());
+      if (ppt <= 16) return f(std::integral_constant<int, 16>());
+      return f(std::integral_constant<int, 32>());
+   }
+   template <class F> static gpe_status with_L(int L, F f) {
+      if (L >= 16) return f(std::integral_constant<int, 16>());
+      if (L == 8) return f(std::integral_constant<int, 8>());
+      if (L == 4) return f(std::integral_constant<int, 4>());
+      return f(std::integral_constant<int, 2>());
+   }
+   template <class F> static gpe_status with_mseg(int m, F f) {
+      if constexpr (std::is_same<R, float>::value && !CPLX)
+         if (m > 16) return f(std::integral_constant<int, 32>());
+      if (m > 8) return f(std::integral_constant<int, 16>());
+      return f(std::integral_constant<int, 8>());
+   }
+
+   static gpe_status run(const Group &G, cudaStream_t st, long long *kernels) {
+      const BatchGeom &A = G.geo;
+      const int n = (int) G.members.size();
+      const BatchDesc *tab = G.dtab;
+      auto S = [&](int q) { return (const int *) (G.dstart + (size_t) q * (n + 1)); };
+      auto T = [&](int q) { return (unsigned) A.tiles[q]; };
+      constexpr int ZL = 8;
+      BCKS(with_ppt(A.zppt, [&](auto pc) {
+         constexpr int PPT = decltype(pc)::value;
+         return launch(kb_zfwd<R, CPLX, PPT, ZL>, T(kPZfwd), A.threads[kPZfwd], A.smem[kPZfwd], st, tab, S(kPZfwd), n);
+      }));
+      BCKS(with_L(G.Ly, [&](auto lc) {
+         constexpr int L = decltype(lc)::value;
+         return launch(kb_yfft<R, false, L>, T(kPYfft), A.threads[kPYfft], A.smem[kPYfft], st, tab, S(kPYfft), n);
+      }));
+      BCKS(with_L(G.Lx, [&](auto lc) {
+         constexpr int L = decltype(lc)::value;
+         return launch(kb_xconv<R, L>, T(kPXconv), A.threads[kPXconv], A.smem[kPXconv], st, tab, S(kPXconv), n);
+      }));
+      BCKS(with_L(G.Ly, [&](auto lc) {
+         constexpr int L = decltype(lc)::value;
+         return launch(kb_yfft<R, true, L>, T(kPYinv), A.threads[kPYinv], A.smem[kPYinv], st, tab, S(kPYinv), n);
+      }));
+      BCKS(with_ppt(A.zppt, [&](auto pc) {
+         constexpr int PPT = decltype(pc)::value;
+         return launch(kb_zinv<R, PPT, ZL>, T(kPZinv), A.threads[kPZinv], A.smem[kPZinv], st, tab, S(kPZinv), n);
+      }));
+      BCKS(launch(kb_phifix<R>, T(kPPhifix), A.threads[kPPhifix], 0, st, tab, S(kPPhifix), n));
+      BCKS(with_mseg(A.mseg[0], [&](auto mc) {
+         constexpr int M = decltype(mc)::value;
+         return launch(kb_sweep_xy<R, CPLX, 0, true, M, 2>, (unsigned) G.sweep_grid[0], A.threads[kPXsweep],
+                       G.sweep_smem[0], st, tab, S(kPXsweep), n, (int) A.tiles[kPXsweep], A.stage[0], A.blk[0]);
+      }));
+      BCKS(with_mseg(A.mseg[1], [&](auto mc) {
+         constexpr int M = decltype(mc)::value;
+         return launch(kb_sweep_xy<R, CPLX, 1, false, M, 2>, (unsigned) G.sweep_grid[1], A.threads[kPYsweep],
+                       G.sweep_smem[1], st, tab, S(kPYsweep), n, (int) A.tiles[kPYsweep], A.stage[1], A.blk[1]);
+      }));
+      BCKS(with_mseg(A.mseg[2], [&](auto mc) {
+         constexpr int M = decltype(mc)::value;
+         constexpr int MOM = CPLX ? 0 : 1;
+         return launch(kb_sweep_z<R, CPLX, MOM, M, 2>, (unsigned) G.sweep_grid[2], A.threads[kPZsweep],
+                       G.sweep_smem[2], st, tab, S(kPZsweep), n, (int) A.tiles[kPZsweep], A.stage[2], A.blk[2],
+                       A.part);
+      }));
+      if (!CPLX) BCKS(launch(kb_norm_final, T(kPNorm), A.threads[kPNorm], 0, st, tab, S(kPNorm), n));
+      *kernels += CPLX ? 9 : 10;
+      return GPE_OK;
+   }
+};
+
+gpe_status queue_step(gpe_batch *b, cudaStream_t st, long long *kernels) {
+   for (const Group &G : b->groups) {
+      if (G.fp32) BCKS(G.cplx ? BatchStep<float, true>::run(G, st, kernels) : BatchStep<float, false>::run(G, st, kernels));
+      else BCKS(G.cplx ? BatchStep<double, true>::run(G, st, kernels) : BatchStep<double, false>::run(G, st, kernels));
+   }
+   return GPE_OK;
+}
+
+// Captures one batch step (every group's passes) on the master stream.
 gpe_status capture(gpe_batch *b) {
    drop_graph(b);
    BCK(cudaSetDevice(b->dev));
-   for (gpe_solver *s : b->inst) BCK(cudaStreamSynchronize(gpe::stream_of(s)));
-   BCK(cudaStreamBeginCapture(b->master, cudaStreamCaptureModeRelaxed));
-   gpe_status st = GPE_OK;
-   cudaError_t e = cudaEventRecord(b->fork, b->master);
-   long long kernels = 0;
-   for (size_t i = 0; i < b->inst.size() && e == cudaSuccess && st == GPE_OK; i++) {
-      cudaStream_t si = gpe::stream_of(b->inst[i]);
-      e = cudaStreamWaitEvent(si, b->fork, 0);
-      if (e != cudaSuccess) break;
-      st = gpe::queue_steps(b->inst[i], 1, b->g[i], b->gd[i]);
-      kernels += gpe::kernels_per_step(b->inst[i]);
-      if (st == GPE_OK) e = cudaEventRecord(b->join[i], si);
-      if (e == cudaSuccess && st == GPE_OK) e = cudaStreamWaitEvent(b->master, b->join[i], 0);
+   if (!b->tables) BCKS(build_tables(b));
+   // the instances' own queued work comes first
+   for (gpe_solver *s : b->inst) {
+      BCK(cudaEventRecord(b->fork, gpe::stream_of(s)));
+      BCK(cudaStreamWaitEvent(b->master, b->fork, 0));
    }
+   BCK(cudaStreamSynchronize(b->master));
+   BCK(cudaStreamBeginCapture(b->master, cudaStreamCaptureModeRelaxed));
+   long long kernels = 0;
+   gpe_status st = queue_step(b, b->master, &kernels);
    cudaGraph_t graph = nullptr;
-   cudaError_t e2 = cudaStreamEndCapture(b->master, &graph);
+   cudaError_t e = cudaStreamEndCapture(b->master, &graph);
    if (st != GPE_OK) {
       if (graph) cudaGraphDestroy(graph);
       return st;
    }
-   if (e != cudaSuccess || e2 != cudaSuccess) {
+   if (e != cudaSuccess) {
       if (graph) cudaGraphDestroy(graph);
-      return bfail(GPE_ERR_CUDA, std::string("batch step capture: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+      return bfail(GPE_ERR_CUDA, std::string("batch step capture: ") + cudaGetErrorString(e));
    }
    b->graph = graph;
    BCK(cudaGraphInstantiate(&b->exec, b->graph, 0));
    b->kernels_per_step = kernels;
+   return GPE_OK;
+}
+
+// Orders the master stream after every instance's queued work.
+gpe_status fan_in(gpe_batch *b) {
+   for (gpe_solver *s : b->inst) {
+      BCK(cudaEventRecord(b->fork, gpe::stream_of(s)));
+      BCK(cudaStreamWaitEvent(b->master, b->fork, 0));
+   }
    return GPE_OK;
 }
 
@@ -117,11 +338,9 @@ extern "C" gpe_status gpe_batch_create(const gpe_params *params, const double *g
          if (gpe::device_of(s) != b->dev) st = bfail(GPE_ERR_PARAM, "batch: all instances must use one device");
    }
    if (st == GPE_OK) e = cudaSetDevice(b->dev);
+   if (st == GPE_OK && e == cudaSuccess) e = cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, b->dev);
    if (st == GPE_OK && e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->master, cudaStreamNonBlocking);
    if (st == GPE_OK && e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
-   b->join.assign(b->inst.size(), nullptr);
-   for (size_t i = 0; i < b->join.size() && st == GPE_OK && e == cudaSuccess; i++)
-      e = cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming);
    if (st == GPE_OK && e != cudaSuccess) st = bfail(GPE_ERR_CUDA, cudaGetErrorString(e));
    if (st != GPE_OK) {
       const std::string keep = gpe_last_error();
@@ -137,10 +356,8 @@ extern "C" void gpe_batch_destroy(gpe_batch *b) {
    if (!b) return;
    if (!b->inst.empty()) cudaSetDevice(b->dev);
    if (b->master) cudaStreamSynchronize(b->master);
-   drop_graph(b);
+   drop_tables(b);
    for (gpe_solver *s : b->inst) gpe_destroy(s);
-   for (cudaEvent_t e : b->join)
-      if (e) cudaEventDestroy(e);
    if (b->fork) cudaEventDestroy(b->fork);
    if (b->master) cudaStreamDestroy(b->master);
    delete b;
@@ -156,13 +373,22 @@ extern "C" gpe_status gpe_batch_set_couplings(gpe_batch *b, const double *g, con
    if (!b || !g || !gd) return bfail(GPE_ERR_PARAM, "batch: null argument");
    b->g.assign(g, g + b->inst.size());
    b->gd.assign(gd, gd + b->inst.size());
-   drop_graph(b);
+   if (!b->tables) return GPE_OK;
+   // rewrite the descriptor tables in place, in stream order after any batch
+   // step already queued; the captured graph reads them at run time
+   BCK(cudaSetDevice(b->dev));
+   for (const Group &G : b->groups) {
+      std::vector<BatchDesc> h;
+      BCKS(group_descs(b, G, h));
+      BCK(cudaMemcpyAsync(G.dtab, h.data(), sizeof(BatchDesc) * h.size(), cudaMemcpyHostToDevice, b->master));
+      BCK(cudaStreamSynchronize(b->master));
+   }
    return GPE_OK;
 }
 
 extern "C" gpe_status gpe_batch_autotune(gpe_batch *b, int nsteps) {
    if (!b) return bfail(GPE_ERR_PARAM, "batch: null handle");
-   drop_graph(b);
+   drop_tables(b);
    // one autotuned representative per (grid, mode, precision)
    std::map<std::tuple<long, long, long, int, int>, gpe_tuning> done;
    for (size_t i = 0; i < b->inst.size(); i++) {
@@ -189,22 +415,13 @@ extern "C" gpe_status gpe_batch_run(gpe_batch *b, long nsteps) {
    if (!b || nsteps < 0) return bfail(GPE_ERR_PARAM, "batch: null handle or negative step count");
    BCK(cudaSetDevice(b->dev));
    if (nsteps == 0) return GPE_OK;
-   if (!b->exec) {
-      gpe_status st = capture(b);
-      if (st != GPE_OK) return st;
-   }
+   if (!b->exec) BCKS(capture(b));
+   BCKS(fan_in(b));
    for (long c = 0; c < nsteps; c++) BCK(cudaGraphLaunch(b->exec, b->master));
    b->launches += b->kernels_per_step * nsteps;
-   gpe_status st = fan_out(b);
-   if (st != GPE_OK) return st;
-   for (gpe_solver *s : b->inst) {
-      st = gpe::queue_finish(s);
-      if (st != GPE_OK) return st;
-   }
-   for (gpe_solver *s : b->inst) {
-      st = gpe_synchronize(s);
-      if (st != GPE_OK) return st;
-   }
+   BCKS(fan_out(b));
+   for (gpe_solver *s : b->inst) BCKS(gpe::queue_finish(s));
+   for (gpe_solver *s : b->inst) BCKS(gpe_synchronize(s));
    BCK(cudaStreamSynchronize(b->master));
    return GPE_OK;
 }
@@ -212,10 +429,8 @@ extern "C" gpe_status gpe_batch_run(gpe_batch *b, long nsteps) {
 extern "C" gpe_status gpe_batch_time_steps(gpe_batch *b, long nsteps, double *ms) {
    if (!b || nsteps < 1) return bfail(GPE_ERR_PARAM, "batch: null handle or nsteps < 1");
    BCK(cudaSetDevice(b->dev));
-   if (!b->exec) {
-      gpe_status st = capture(b);
-      if (st != GPE_OK) return st;
-   }
+   if (!b->exec) BCKS(capture(b));
+   BCKS(fan_in(b));
    cudaEvent_t e0, e1;
    BCK(cudaEventCreate(&e0));
    BCK(cudaEventCreate(&e1));

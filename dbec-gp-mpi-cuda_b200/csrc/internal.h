@@ -25,4 +25,13 @@ gpe_status params_of(gpe_solver *s, gpe_params *p);
 int device_of(gpe_solver *s);
 long long kernels_per_step(gpe_solver *s);
 
+// Batched launches (batch.cu): the instance's launch geometry under the
+// batch's tile choices with y / x FFT tiles of Ly / Lx columns (Ly = Lx = 0:
+// only geom->Ly / Lx, the instance's own widths, are filled in), and its
+// descriptor with those tiles and couplings g, gd.
+struct BatchDesc;
+struct BatchGeom;
+gpe_status batch_geom(gpe_solver *s, int Ly, int Lx, BatchGeom *geom);
+gpe_status batch_desc(gpe_solver *s, int Ly, int Lx, double g, double gd, BatchDesc *out);
+
 }  // namespace gpe

@@ -19,6 +19,7 @@
 #include "internal.h"
 #include "step_kernels.cuh"
 #include "sweep_kernels.cuh"
+#include "batch_kernels.cuh"
 
 using namespace gpe;
 
@@ -1011,6 +1012,127 @@ template <class R, bool CPLX> struct Impl {
    }
 
    static gpe_status density(gpe_solver *s, int kind, long sx, long sy, long sz, double *out, long cap, long *count);
+
+   // ---- batched launches: geometry and descriptor of this instance
+   static gpe_status geom(gpe_solver *s, int Ly, int Lx, BatchGeom *g) {
+      const Dims &d = s->d;
+      *g = BatchGeom{};
+      g->Ly = s->Ly;
+      g->Lx = s->Lx;
+      if (Ly <= 0 || Lx <= 0) return GPE_OK;
+      // z passes: 8-row tiles on CTAs sized to them
+      constexpr int L = 8;
+      const int zp = zppt(s, L);
+      const int ppt = zp <= 8 ? 8 : (zp <= 16 ? 16 : 32);
+      g->zppt = ppt;
+      g->tiles[kPZfwd] = g->tiles[kPZinv] = (d.nxy + L - 1) / L;
+      g->threads[kPZfwd] = g->threads[kPZinv] = z_threads(s, L, ppt);
+      g->smem[kPZfwd] = zfwd_smem(s, L);
+      g->smem[kPZinv] = zinv_smem(s, L);
+      if (g->smem[kPZfwd] > 227 * 1024 || g->smem[kPZinv] > 227 * 1024)
+         return fail(GPE_ERR_PARAM, "batch: z rows too long for 8-row tiles");
+      // y / x passes
+      const long ry = (long) s->boxy * s->nboxy, rx = (long) s->boxx * s->nboxx;
+      if (ry * Ly > 256L * FftL<R>::PPT || rx * Lx > 256L * FftL<R>::PPT)
+         return fail(GPE_ERR_PARAM, "batch: FFT tile too wide for this grid");
+      g->tiles[kPYfft] = g->tiles[kPYinv] = (long long) d.nx * ((d.nzh + Ly - 1) / Ly);
+      g->tiles[kPXconv] = (long long) d.ny * ((d.nzh + Lx - 1) / Lx);
+      g->threads[kPYfft] = g->threads[kPYinv] = fft_threads(ry, Ly);
+      g->threads[kPXconv] = fft_threads(rx, Lx);
+      g->smem[kPYfft] = g->smem[kPYinv] = 128 + (size_t) ry * Ly * sizeof(C) + d.ny * sizeof(C);
+      g->smem[kPXconv] = 128 + (size_t) rx * Lx * sizeof(C) + d.nx * sizeof(C) + (size_t) (d.nx / 2 + 1) * Lx * sizeof(double);
+      // boundary planes of phi
+      g->tiles[kPPhifix] = std::max<long>(1, (d.ny - 1) + (d.nx - 1));
+      g->threads[kPPhifix] = (unsigned) std::min<long>(256, std::max<long>(32, (d.nz - 1 + 31) / 32 * 32));
+      // sweeps
+      const size_t esz = s->esz_psi;
+      for (int ax = 0; ax < 3; ax++) {
+         const auto &w = s->sw[ax];
+         const int TW = w.TW, P = w.tab.P, spw = 32 / TW;
+         const int kp = kPXsweep + ax;
+         g->mseg[ax] = w.MSEG;
+         g->threads[kp] = (unsigned) ((TW * P + 31) & ~31);
+         const int nzb = (d.nz + TW - 1) / TW;
+         g->tiles[kp] = ax == 0 ? (long long) d.ny * nzb : (ax == 1 ? (long long) d.nx * nzb : (d.nxy + TW - 1) / TW);
+         size_t stage;
+         if (ax < 2) {
+            const size_t rows = (size_t) w.boxn * w.nbox;
+            stage = rows * TW * esz + (ax == 0 ? rows * TW * s->esz_r : 0);
+         } else {
+            stage = (size_t) TW * w.LS * esz;
+         }
+         g->stage[ax] = (uint32_t) ((stage + 127) & ~(size_t) 127);
+         g->blk[ax] = (uint32_t) ((2 * (size_t) ((P + spw - 1) / spw + 1) * TW * esz + 15) & ~(size_t) 15);
+         if (!s->fp32) {
+            if (ax == 0) g->extra[ax] = (uint32_t) (d.nx * sizeof(double));
+            if (ax == 2) g->extra[ax] = (uint32_t) (4 * (size_t) d.nz * (s->cplx ? 16 : 8));
+         }
+         if (ax == 2) g->part = (uint32_t) (((size_t) P * TW * sizeof(double) + 15) & ~(size_t) 15);
+      }
+      // norm (imaginary time)
+      g->tiles[kPNorm] = s->cplx ? 0 : (d.nx + kNormRowsPerCta - 1) / kNormRowsPerCta;
+      g->threads[kPNorm] = 32 * kNormRowsPerCta;
+      return GPE_OK;
+   }
+
+   static gpe_status desc(gpe_solver *s, int Ly, int Lx, double g, double gd, BatchDesc *D) {
+      const Dims &d = s->d;
+      std::memset((void *) D, 0, sizeof(BatchDesc));
+      D->tm_psi[0] = s->sw[0].tm_psi;
+      D->tm_psi[1] = s->sw[1].tm_psi;
+      D->tm_phi = s->sw[0].tm_phi;
+      CKS(make_tmap(&D->tm_spec_y, s->spec, s->esz_r, 2 * d.nzh, d.ny, d.nx, 2 * Ly, s->boxy, 1, 2 * d.nzp));
+      CKS(make_tmap(&D->tm_spec_x, s->spec, s->esz_r, 2 * d.nzh, d.ny, d.nx, 2 * Lx, 1, s->boxx, 2 * d.nzp));
+      for (int ax = 0; ax < 3; ax++) {
+         const auto &w = s->sw[ax];
+         SweepView &v = D->sv[ax];
+         v.tb = w.tab;
+         v.trap = trap_of(s);
+         v.lin = LinPhase{s->lin[0], s->lin[1], s->lin[2]};
+         v.d = d;
+         v.st = s->state;
+         v.err = s->err;
+         v.psi = s->psi;
+         v.wz = s->wz;
+         v.wz2 = s->wz2;
+         v.rowsum = s->rowA;
+         v.rowsum2 = s->rowB;
+         v.g = g;
+         v.gd = gd;
+         v.dt = s->p.dt;
+         v.hz3 = s->p.dz / 3.;
+         v.TW = w.TW;
+         v.boxn = w.boxn;
+         v.nbox = w.nbox;
+         v.LS = w.LS;
+      }
+      D->px = s->px;
+      D->py = s->py;
+      D->ph = s->ph;
+      D->d = d;
+      D->psi = s->psi;
+      D->spec = s->spec;
+      D->phi = s->phi;
+      D->twx = s->twx;
+      D->twy = s->twy;
+      D->twz = s->twz;
+      D->udd = s->udd;
+      D->state = s->state;
+      D->err = s->err;
+      D->rowA = s->rowA;
+      D->xs = s->tmp;
+      D->hx = s->p.dx;
+      D->hy = s->p.dy;
+      D->LSr = s->LSr;
+      D->LSo = s->LSo;
+      D->boxy = s->boxy;
+      D->nboxy = s->nboxy;
+      D->boxx = s->boxx;
+      D->nboxx = s->nboxx;
+      D->Ly = Ly;
+      D->Lx = Lx;
+      return GPE_OK;
+   }
 };
 
 template <class R, bool CPLX>
@@ -1677,6 +1799,16 @@ gpe_status params_of(gpe_solver *s, gpe_params *p) {
 }
 int device_of(gpe_solver *s) { return s->dev; }
 long long kernels_per_step(gpe_solver *s) { return s->cplx ? 9 : 10; }
+
+gpe_status batch_geom(gpe_solver *s, int Ly, int Lx, BatchGeom *geom) {
+   CHECK_HANDLE(s);
+   return DISPATCH(s, geom(s, Ly, Lx, geom));
+}
+
+gpe_status batch_desc(gpe_solver *s, int Ly, int Lx, double g, double gd, BatchDesc *out) {
+   CHECK_HANDLE(s);
+   return DISPATCH(s, desc(s, Ly, Lx, g, gd, out));
+}
 
 }  // namespace gpe
 

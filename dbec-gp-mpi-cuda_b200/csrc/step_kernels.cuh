@@ -359,7 +359,7 @@ __global__ void k_phifix(R *__restrict__ phi, Dims d) {
 // nothing is in flight when the wait gives up after `spins` polls; the CTA
 // then leaves together, exactly as a step kernel whose tile never arrived,
 // and the handle's status word reports the timeout.
-__global__ void k_wait_selftest(uint32_t spins, uint32_t *err) {
+static __global__ void k_wait_selftest(uint32_t spins, uint32_t *err) {
    __shared__ __align__(8) uint64_t bar;
    if (threadIdx.x == 0) {
       mbar_init(&bar, 1);
@@ -475,7 +475,7 @@ __device__ __forceinline__ void norm_final_body(const double *__restrict__ rowsu
    }
 }
 
-__global__ void __launch_bounds__(32 * kNormRowsPerCta) k_norm_final(const double *__restrict__ rowsum, Dims d,
+static __global__ void __launch_bounds__(32 * kNormRowsPerCta) k_norm_final(const double *__restrict__ rowsum, Dims d,
                                                                      double hx, double hy, State *st, double *xs,
                                                                      double *out_norm) {
    pdl_trigger();
@@ -491,7 +491,7 @@ __global__ void k_apply_scale(typename Tr<R, CPLX>::P *__restrict__ psi, long lo
       psi[q] = scl(psi[q], s);
 }
 
-__global__ void k_state_set(State *st, double scale) {
+static __global__ void k_state_set(State *st, double scale) {
    st->scale = scale;
    st->scale2 = scale * scale;
 }
@@ -501,7 +501,7 @@ __global__ void k_state_set(State *st, double scale) {
 // S_x S_y y^2 rowA, <z^2> = S_x S_y rowB; out = (r, rx, ry, rz).  Each warp
 // forms the three weighted Simpson sums over y of one x row into xs[3 nx];
 // the last CTA to finish integrates them over x.
-__global__ void __launch_bounds__(32 * kNormRowsPerCta) k_rms_final(const double *__restrict__ rowA,
+static __global__ void __launch_bounds__(32 * kNormRowsPerCta) k_rms_final(const double *__restrict__ rowA,
                                                                     const double *__restrict__ rowB, Dims d, double hx,
                                                                     double hy, const double *__restrict__ x2,
                                                                     const double *__restrict__ y2, State *st,
@@ -555,7 +555,7 @@ __global__ void __launch_bounds__(32 * kNormRowsPerCta) k_rms_final(const double
 }
 
 // Generic S_x S_y of a per-row array (mu, E, norm).
-__global__ void k_xy_final(const double *__restrict__ rowA, Dims d, double hx, double hy, double *__restrict__ out) {
+static __global__ void k_xy_final(const double *__restrict__ rowA, Dims d, double hx, double hy, double *__restrict__ out) {
    extern __shared__ double tx[];
    for (int i = threadIdx.x; i < d.nx; i += blockDim.x) tx[i] = simpint_arr(hy, rowA + (long long) i * d.ny, d.ny);
    __syncthreads();
@@ -631,7 +631,7 @@ __global__ void k_lineint_psi(const typename Tr<R, CPLX>::P *__restrict__ psi, D
 }
 
 // out[u] = Simpson along axis `ax` (0 rows, 1 columns) of a [n0][n1] array.
-__global__ void k_lineint_arr(const double *__restrict__ a, int n0, int n1, int ax, double h, double *__restrict__ out) {
+static __global__ void k_lineint_arr(const double *__restrict__ a, int n0, int n1, int ax, double h, double *__restrict__ out) {
    const int l = blockIdx.x * blockDim.x + threadIdx.x;
    if (ax == 1) {
       if (l < n0) out[l] = simpint_arr(h, a + (long long) l * n1, n1, 1);

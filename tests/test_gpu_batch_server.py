@@ -89,7 +89,9 @@ def test_batch_equals_individual_runs(gpe_lib):
             s.calcnorm(True)
     b.run(12)
     b.run(3)
-    assert b.launch_count() == 15 * sum(10 if p.mode == 0 else 9 for p in ps)
+    # one launch per pass and group: 10 passes for the imaginary-time group,
+    # 9 for the real-time one
+    assert b.launch_count() == 15 * (10 + 9)
     for i, p in enumerate(ps):
         s = gpe.Solver(p)
         s.init_gaussian()
@@ -97,6 +99,43 @@ def test_batch_equals_individual_runs(gpe_lib):
             s.calcnorm(True)
         s.run(12, g[i], gd[i])
         s.run(3, g[i], gd[i])
+        assert np.array_equal(s.get_psi(), b.solver(i).get_psi()), i
+        s.close()
+    b.close()
+
+
+def test_batch_groups_and_new_couplings_bitwise(gpe_lib):
+    """Four groups (both modes, both precisions), grids whose sweeps use
+    different segment lengths and tiles (48^3 .. 128^3, uneven shapes),
+    couplings changed between runs (the descriptor table is rewritten, the
+    captured step stays): every instance equals its own solo run bit for bit."""
+    gpe = gpe_lib
+    ps = [params(gpe, 0, (48, 48, 48), prec=1), params(gpe, 0, (96, 96, 64), dx=0.2, prec=1),
+          params(gpe, 1, (48, 40, 32), dx=0.2, dt=4e-4, trap=(1., 1., 4.), prec=1),
+          params(gpe, 0, (64, 64, 64), prec=0), params(gpe, 1, (32, 32, 32), dt=5e-4, prec=0),
+          params(gpe, 0, (24, 20, 32), dx=0.3, trap=(1., 0.7, 2.), prec=1),
+          params(gpe, 0, (128, 128, 128), dx=0.2, prec=1), params(gpe, 1, (40, 48, 64), dt=4e-4, prec=1),
+          params(gpe, 0, (80, 64, 48), dx=0.2, prec=0)]
+    g = [100., 60., 40., 80., 50., 30., 150., 70., 90.]
+    gd = [30., 20., 10., 50., 5., 3., 40., 15., 25.]
+    g2 = [x * 1.5 for x in g]
+    gd2 = [x * 0.5 for x in gd]
+    b = gpe.Batch(ps, g, gd)
+    for i, p in enumerate(ps):
+        s = b.solver(i)
+        s.init_gaussian()
+        if p.mode == 0:
+            s.calcnorm(True)
+    b.run(7)
+    b.set_couplings(g2, gd2)
+    b.run(5)
+    for i, p in enumerate(ps):
+        s = gpe.Solver(p)
+        s.init_gaussian()
+        if p.mode == 0:
+            s.calcnorm(True)
+        s.run(7, g[i], gd[i])
+        s.run(5, g2[i], gd2[i])
         assert np.array_equal(s.get_psi(), b.solver(i).get_psi()), i
         s.close()
     b.close()
