@@ -35,9 +35,9 @@ struct Group {
    std::vector<int> members;  // instance indices
    int Ly = 0, Lx = 0;        // FFT tile widths (the narrowest of the members)
    BatchGeom geo{};           // maxima over the members (tiles: sums)
-   std::vector<int> start;    // [kNPass][n + 1] tile offsets
-   BatchDesc *dtab = nullptr; // device descriptor table
-   int *dstart = nullptr;     // device copy of start
+   long long off[kNPass + 1] = {};  // start of each pass's work list in dwork
+   BatchDesc *dtab = nullptr;        // device descriptor table
+   unsigned *dwork = nullptr;        // device work lists (TileRef packed per tile)
    int sweep_grid[3] = {0, 0, 0};
    size_t sweep_smem[3] = {0, 0, 0};
 };
@@ -88,7 +88,7 @@ void drop_tables(gpe_batch *b) {
    drop_graph(b);
    for (Group &G : b->groups) {
       if (G.dtab) cudaFree(G.dtab);
-      if (G.dstart) cudaFree(G.dstart);
+      if (G.dwork) cudaFree(G.dwork);
    }
    b->groups.clear();
    b->tables = false;
@@ -134,14 +134,15 @@ gpe_status build_tables(gpe_batch *b) {
          G.Ly = std::min(G.Ly, own.Ly);
          G.Lx = std::min(G.Lx, own.Lx);
       }
-      G.start.assign((size_t) kNPass * (n + 1), 0);
+      if (n > (1 << kInstBits)) return bfail(GPE_ERR_PARAM, "batch: at most 4096 instances of one mode and precision");
       BatchGeom &A = G.geo;
       A = BatchGeom{};
+      std::vector<BatchGeom> geo(n);
       for (int k = 0; k < n; k++) {
-         BatchGeom g;
+         BatchGeom &g = geo[k];
          BCKS(gpe::batch_geom(b->inst[G.members[k]], G.Ly, G.Lx, &g));
          for (int q = 0; q < kNPass; q++) {
-            G.start[(size_t) q * (n + 1) + k + 1] = G.start[(size_t) q * (n + 1) + k] + (int) g.tiles[q];
+            if (g.tiles[q] > (1LL << kLocalBits)) return bfail(GPE_ERR_PARAM, "batch: too many tiles in one instance");
             A.tiles[q] += g.tiles[q];
             A.threads[q] = std::max(A.threads[q], g.threads[q]);
             A.smem[q] = std::max(A.smem[q], g.smem[q]);
@@ -168,12 +169,21 @@ gpe_status build_tables(gpe_batch *b) {
          G.sweep_smem[a] = sm;
          G.sweep_grid[a] = (int) std::min<long long>(A.tiles[kPXsweep + a], (long long) ctas * b->nsm);
       }
+      // work lists: every pass's tiles, instance by instance
+      G.off[0] = 0;
+      for (int q = 0; q < kNPass; q++) G.off[q + 1] = G.off[q] + A.tiles[q];
+      std::vector<unsigned> work((size_t) G.off[kNPass]);
+      for (int q = 0; q < kNPass; q++) {
+         size_t e = (size_t) G.off[q];
+         for (int k = 0; k < n; k++)
+            for (long long t = 0; t < geo[k].tiles[q]; t++) work[e++] = ((unsigned) k << kLocalBits) | (unsigned) t;
+      }
       std::vector<BatchDesc> h;
       BCKS(group_descs(b, G, h));
       BCK(cudaMalloc(&G.dtab, sizeof(BatchDesc) * h.size()));
-      BCK(cudaMalloc(&G.dstart, sizeof(int) * G.start.size()));
+      BCK(cudaMalloc(&G.dwork, sizeof(unsigned) * std::max<size_t>(1, work.size())));
       BCK(cudaMemcpyAsync(G.dtab, h.data(), sizeof(BatchDesc) * h.size(), cudaMemcpyHostToDevice, b->master));
-      BCK(cudaMemcpyAsync(G.dstart, G.start.data(), sizeof(int) * G.start.size(), cudaMemcpyHostToDevice, b->master));
+      BCK(cudaMemcpyAsync(G.dwork, work.data(), sizeof(unsigned) * work.size(), cudaMemcpyHostToDevice, b->master));
    }
    BCK(cudaStreamSynchronize(b->master));
    b->tables = true;
@@ -211,61 +221,80 @@ template <class R, bool CPLX> struct BatchStep {
       return f(std::integral_constant<int, 8>());
    }
 
-   static gpe_status run(const Group &G, cudaStream_t st, long long *kernels) {
+   // ev (may be null): an event recorded after every pass, index = pass
+   static gpe_status run(const Group &G, cudaStream_t st, long long *kernels, cudaEvent_t *ev = nullptr) {
       const BatchGeom &A = G.geo;
-      const int n = (int) G.members.size();
       const BatchDesc *tab = G.dtab;
-      auto S = [&](int q) { return (const int *) (G.dstart + (size_t) q * (n + 1)); };
+      auto S = [&](int q) { return (const unsigned *) (G.dwork + G.off[q]); };
       auto T = [&](int q) { return (unsigned) A.tiles[q]; };
       constexpr int ZL = 8;
+      auto mark = [&](int q) -> gpe_status {
+         if (ev) BCK(cudaEventRecord(ev[q], st));
+         return GPE_OK;
+      };
       BCKS(with_ppt(A.zppt, [&](auto pc) {
          constexpr int PPT = decltype(pc)::value;
-         return launch(kb_zfwd<R, CPLX, PPT, ZL>, T(kPZfwd), A.threads[kPZfwd], A.smem[kPZfwd], st, tab, S(kPZfwd), n);
+         return launch(kb_zfwd<R, CPLX, PPT, ZL>, T(kPZfwd), A.threads[kPZfwd], A.smem[kPZfwd], st, tab, S(kPZfwd));
       }));
+      BCKS(mark(kPZfwd));
       BCKS(with_L(G.Ly, [&](auto lc) {
          constexpr int L = decltype(lc)::value;
-         return launch(kb_yfft<R, false, L>, T(kPYfft), A.threads[kPYfft], A.smem[kPYfft], st, tab, S(kPYfft), n);
+         return launch(kb_yfft<R, false, L>, T(kPYfft), A.threads[kPYfft], A.smem[kPYfft], st, tab, S(kPYfft));
       }));
+      BCKS(mark(kPYfft));
       BCKS(with_L(G.Lx, [&](auto lc) {
          constexpr int L = decltype(lc)::value;
-         return launch(kb_xconv<R, L>, T(kPXconv), A.threads[kPXconv], A.smem[kPXconv], st, tab, S(kPXconv), n);
+         return launch(kb_xconv<R, L>, T(kPXconv), A.threads[kPXconv], A.smem[kPXconv], st, tab, S(kPXconv));
       }));
+      BCKS(mark(kPXconv));
       BCKS(with_L(G.Ly, [&](auto lc) {
          constexpr int L = decltype(lc)::value;
-         return launch(kb_yfft<R, true, L>, T(kPYinv), A.threads[kPYinv], A.smem[kPYinv], st, tab, S(kPYinv), n);
+         return launch(kb_yfft<R, true, L>, T(kPYinv), A.threads[kPYinv], A.smem[kPYinv], st, tab, S(kPYinv));
       }));
+      BCKS(mark(kPYinv));
       BCKS(with_ppt(A.zppt, [&](auto pc) {
          constexpr int PPT = decltype(pc)::value;
-         return launch(kb_zinv<R, PPT, ZL>, T(kPZinv), A.threads[kPZinv], A.smem[kPZinv], st, tab, S(kPZinv), n);
+         return launch(kb_zinv<R, PPT, ZL>, T(kPZinv), A.threads[kPZinv], A.smem[kPZinv], st, tab, S(kPZinv));
       }));
-      BCKS(launch(kb_phifix<R>, T(kPPhifix), A.threads[kPPhifix], 0, st, tab, S(kPPhifix), n));
+      BCKS(mark(kPZinv));
+      BCKS(launch(kb_phifix<R>, T(kPPhifix), A.threads[kPPhifix], 0, st, tab, S(kPPhifix)));
+      BCKS(mark(kPPhifix));
       BCKS(with_mseg(A.mseg[0], [&](auto mc) {
          constexpr int M = decltype(mc)::value;
          return launch(kb_sweep_xy<R, CPLX, 0, true, M, 2>, (unsigned) G.sweep_grid[0], A.threads[kPXsweep],
-                       G.sweep_smem[0], st, tab, S(kPXsweep), n, (int) A.tiles[kPXsweep], A.stage[0], A.blk[0]);
+                       G.sweep_smem[0], st, tab, S(kPXsweep), (int) A.tiles[kPXsweep], A.stage[0], A.blk[0]);
       }));
+      BCKS(mark(kPXsweep));
       BCKS(with_mseg(A.mseg[1], [&](auto mc) {
          constexpr int M = decltype(mc)::value;
          return launch(kb_sweep_xy<R, CPLX, 1, false, M, 2>, (unsigned) G.sweep_grid[1], A.threads[kPYsweep],
-                       G.sweep_smem[1], st, tab, S(kPYsweep), n, (int) A.tiles[kPYsweep], A.stage[1], A.blk[1]);
+                       G.sweep_smem[1], st, tab, S(kPYsweep), (int) A.tiles[kPYsweep], A.stage[1], A.blk[1]);
       }));
+      BCKS(mark(kPYsweep));
       BCKS(with_mseg(A.mseg[2], [&](auto mc) {
          constexpr int M = decltype(mc)::value;
          constexpr int MOM = CPLX ? 0 : 1;
          return launch(kb_sweep_z<R, CPLX, MOM, M, 2>, (unsigned) G.sweep_grid[2], A.threads[kPZsweep],
-                       G.sweep_smem[2], st, tab, S(kPZsweep), n, (int) A.tiles[kPZsweep], A.stage[2], A.blk[2],
+                       G.sweep_smem[2], st, tab, S(kPZsweep), (int) A.tiles[kPZsweep], A.stage[2], A.blk[2],
                        A.part);
       }));
-      if (!CPLX) BCKS(launch(kb_norm_final, T(kPNorm), A.threads[kPNorm], 0, st, tab, S(kPNorm), n));
+      BCKS(mark(kPZsweep));
+      if (!CPLX) BCKS(launch(kb_norm_final, T(kPNorm), A.threads[kPNorm], 0, st, tab, S(kPNorm)));
+      BCKS(mark(kPNorm));
       *kernels += CPLX ? 9 : 10;
       return GPE_OK;
    }
 };
 
-gpe_status queue_step(gpe_batch *b, cudaStream_t st, long long *kernels) {
-   for (const Group &G : b->groups) {
-      if (G.fp32) BCKS(G.cplx ? BatchStep<float, true>::run(G, st, kernels) : BatchStep<float, false>::run(G, st, kernels));
-      else BCKS(G.cplx ? BatchStep<double, true>::run(G, st, kernels) : BatchStep<double, false>::run(G, st, kernels));
+// ev (may be null): per group, kNPass events recorded after its passes
+gpe_status queue_step(gpe_batch *b, cudaStream_t st, long long *kernels, cudaEvent_t *ev = nullptr) {
+   for (size_t gi = 0; gi < b->groups.size(); gi++) {
+      const Group &G = b->groups[gi];
+      cudaEvent_t *e = ev ? ev + gi * kNPass : nullptr;
+      if (G.fp32)
+         BCKS(G.cplx ? BatchStep<float, true>::run(G, st, kernels, e) : BatchStep<float, false>::run(G, st, kernels, e));
+      else
+         BCKS(G.cplx ? BatchStep<double, true>::run(G, st, kernels, e) : BatchStep<double, false>::run(G, st, kernels, e));
    }
    return GPE_OK;
 }
@@ -449,6 +478,46 @@ extern "C" gpe_status gpe_batch_time_steps(gpe_batch *b, long nsteps, double *ms
    for (gpe_solver *s : b->inst)
       if (st == GPE_OK) st = gpe_synchronize(s);
    if (ms) *ms = f;
+   return st;
+}
+
+extern "C" gpe_status gpe_batch_profile_step(gpe_batch *b, long nsteps, double *ms, int cap, int *count) {
+   if (!b || !ms || nsteps < 1) return bfail(GPE_ERR_PARAM, "batch: null argument or nsteps < 1");
+   if (cap < kNPass) return bfail(GPE_ERR_PARAM, "batch: profile output array too small");
+   BCK(cudaSetDevice(b->dev));
+   if (!b->tables) BCKS(build_tables(b));
+   BCKS(fan_in(b));
+   const size_t ng = b->groups.size();
+   std::vector<cudaEvent_t> ev((size_t) nsteps * (ng * kNPass + 1));
+   for (auto &e : ev) BCK(cudaEventCreate(&e));
+   long long kernels = 0;
+   gpe_status st = GPE_OK;
+   for (long c = 0; c < nsteps && st == GPE_OK; c++) {
+      cudaEvent_t *base = ev.data() + c * (ng * kNPass + 1);
+      cudaEventRecord(base[0], b->master);
+      st = queue_step(b, b->master, &kernels, base + 1);
+   }
+   cudaError_t e = cudaStreamSynchronize(b->master);
+   if (st == GPE_OK && e != cudaSuccess) st = bfail(GPE_ERR_CUDA, cudaGetErrorString(e));
+   if (st == GPE_OK) {
+      for (int q = 0; q < kNPass; q++) ms[q] = 0.;
+      for (long c = 0; c < nsteps; c++) {
+         cudaEvent_t *base = ev.data() + c * (ng * kNPass + 1);
+         for (size_t k = 0; k < ng * kNPass; k++) {
+            float f = 0.f;
+            cudaEventElapsedTime(&f, base[k], base[k + 1]);
+            ms[k % kNPass] += f / nsteps;
+         }
+      }
+      if (count) *count = kNPass;
+      b->launches += kernels;
+   }
+   for (auto &x : ev) cudaEventDestroy(x);
+   if (st == GPE_OK) st = fan_out(b);
+   for (gpe_solver *s : b->inst)
+      if (st == GPE_OK) st = gpe::queue_finish(s);
+   for (gpe_solver *s : b->inst)
+      if (st == GPE_OK) st = gpe_synchronize(s);
    return st;
 }
 

@@ -8,14 +8,15 @@
 // over the tiles of all instances of a group (same mode and precision): a
 // per-instance descriptor table in device memory holds each instance's
 // dimensions, pointers, FFT plans, coefficient tables, couplings and TMA
-// tensor maps, and a work list (prefix sums of the instances' tile counts)
-// maps a CTA's tile to its instance.  The per-tile arithmetic is the single
+// tensor maps, and a work list per pass maps a tile to its instance and its
+// place in that instance.  The per-tile arithmetic is the single
 // solve's own (the *_body functions of step_kernels.cuh and the sweep helpers
 // of sweep_kernels.cuh), so an instance's step is bit for bit its solo step.
 //
 // Tensor maps read from global memory are acquired through the tensormap
 // proxy (fence.proxy.tensormap::generic.acquire) by the thread that issues
-// the copies, before their first use in the CTA.
+// the copies, before their first use in the CTA (and again whenever a
+// persistent CTA moves on to another instance).
 #pragma once
 
 #include "step_kernels.cuh"
@@ -80,15 +81,17 @@ __device__ __forceinline__ void tmap_acquire(const CUtensorMap *m) {
    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(m) : "memory");
 }
 
-// Instance owning tile t: start[i] <= t < start[i + 1] (start[0] = 0).
-__device__ __forceinline__ int find_inst(const int *__restrict__ start, int n, int t) {
-   int lo = 0, hi = n - 1;
-   while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (__ldg(start + mid) <= t) lo = mid;
-      else hi = mid - 1;
-   }
-   return lo;
+// Work list of a pass: entry t packs the instance owning tile t (high
+// kInstBits bits) and the tile's index within that instance (low bits), so a
+// CTA finds its instance with one load.
+constexpr int kInstBits = 12;
+constexpr int kLocalBits = 32 - kInstBits;
+struct TileRef {
+   int inst, local;
+};
+__device__ __forceinline__ TileRef tile_ref(const unsigned *__restrict__ work, int t) {
+   const unsigned w = __ldg(work + t);
+   return TileRef{(int) (w >> kLocalBits), (int) (w & ((1u << kLocalBits) - 1u))};
 }
 
 // Copies a plan into shared memory (every thread of the CTA calls it); the
@@ -105,73 +108,71 @@ __device__ __forceinline__ void stage_plan(FftPlan &dst, const FftPlan &src) {
 
 template <class R, bool CPLX, int PPT, int L>
 __global__ void __launch_bounds__(256, L >= 16 ? 3 : 4) kb_zfwd(const BatchDesc *__restrict__ tab,
-                                                                const int *__restrict__ start, int n) {
-   const int i = find_inst(start, n, blockIdx.x);
-   const BatchDesc &D = tab[i];
+                                                                const unsigned *__restrict__ work) {
+   const TileRef r = tile_ref(work, blockIdx.x);
+   const BatchDesc &D = tab[r.inst];
    __shared__ FftPlan pl;
    stage_plan(pl, D.ph);
    const Dims d = D.d;
    zfwd_body<R, CPLX, PPT, L>((const typename Tr<R, CPLX>::P *) D.psi, (cpx<R> *) D.spec, d, pl,
-                              (const cpx<R> *) D.twz, D.LSr, D.err, (long long) (blockIdx.x - __ldg(start + i)) * L);
+                              (const cpx<R> *) D.twz, D.LSr, D.err, (long long) r.local * L);
 }
 
 template <class R, bool INV, int L>
-__global__ void __launch_bounds__(256, 4) kb_yfft(const BatchDesc *__restrict__ tab, const int *__restrict__ start,
-                                                  int n) {
-   const int i = find_inst(start, n, blockIdx.x);
-   const BatchDesc &D = tab[i];
+__global__ void __launch_bounds__(256, 4) kb_yfft(const BatchDesc *__restrict__ tab,
+                                                  const unsigned *__restrict__ work) {
+   const TileRef r = tile_ref(work, blockIdx.x);
+   const BatchDesc &D = tab[r.inst];
    __shared__ FftPlan pl;
    if (threadIdx.x == 0) tmap_acquire(&D.tm_spec_y);
    stage_plan(pl, D.py);
    const Dims d = D.d;
-   const int local = blockIdx.x - __ldg(start + i);
    const int nkb = (d.nzh + L - 1) / L;
-   const int x = local / nkb, k0 = (local - x * nkb) * L;
+   const int x = r.local / nkb, k0 = (r.local - x * nkb) * L;
    yfft_body<R, INV, L>(&D.tm_spec_y, d, pl, (const cpx<R> *) D.twy, D.boxy, D.nboxy, D.err, x, k0);
 }
 
 template <class R, int L>
-__global__ void __launch_bounds__(256, 4) kb_xconv(const BatchDesc *__restrict__ tab, const int *__restrict__ start,
-                                                   int n) {
-   const int i = find_inst(start, n, blockIdx.x);
-   const BatchDesc &D = tab[i];
+__global__ void __launch_bounds__(256, 4) kb_xconv(const BatchDesc *__restrict__ tab,
+                                                   const unsigned *__restrict__ work) {
+   const TileRef r = tile_ref(work, blockIdx.x);
+   const BatchDesc &D = tab[r.inst];
    __shared__ FftPlan pl;
    if (threadIdx.x == 0) tmap_acquire(&D.tm_spec_x);
    stage_plan(pl, D.px);
    const Dims d = D.d;
-   const int local = blockIdx.x - __ldg(start + i);
    const int nkb = (d.nzh + L - 1) / L;
-   const int y = local / nkb, k0 = (local - y * nkb) * L;
+   const int y = r.local / nkb, k0 = (r.local - y * nkb) * L;
    xconv_body<R, L>(&D.tm_spec_x, d, pl, (const cpx<R> *) D.twx, D.udd, D.state, D.boxx, D.nboxx, D.err, y, k0);
 }
 
 template <class R, int PPT, int L>
 __global__ void __launch_bounds__(256, L >= 16 ? 3 : 4) kb_zinv(const BatchDesc *__restrict__ tab,
-                                                                const int *__restrict__ start, int n) {
-   const int i = find_inst(start, n, blockIdx.x);
-   const BatchDesc &D = tab[i];
+                                                                const unsigned *__restrict__ work) {
+   const TileRef r = tile_ref(work, blockIdx.x);
+   const BatchDesc &D = tab[r.inst];
    __shared__ FftPlan pl;
    stage_plan(pl, D.ph);
    const Dims d = D.d;
    zinv_body<R, PPT, L>((const cpx<R> *) D.spec, (R *) D.phi, d, pl, (const cpx<R> *) D.twz, D.LSo, D.err,
-                        (long long) (blockIdx.x - __ldg(start + i)) * L);
+                        (long long) r.local * L);
 }
 
 template <class R>
-__global__ void kb_phifix(const BatchDesc *__restrict__ tab, const int *__restrict__ start, int n) {
-   const int i = find_inst(start, n, blockIdx.x);
-   const BatchDesc &D = tab[i];
+__global__ void kb_phifix(const BatchDesc *__restrict__ tab, const unsigned *__restrict__ work) {
+   const TileRef r = tile_ref(work, blockIdx.x);
+   const BatchDesc &D = tab[r.inst];
    const Dims d = D.d;
-   phifix_body<R>((R *) D.phi, d, blockIdx.x - __ldg(start + i));
+   phifix_body<R>((R *) D.phi, d, r.local);
 }
 
 static __global__ void __launch_bounds__(32 * kNormRowsPerCta) kb_norm_final(const BatchDesc *__restrict__ tab,
-                                                                      const int *__restrict__ start, int n) {
-   const int i = find_inst(start, n, blockIdx.x);
-   const BatchDesc &D = tab[i];
+                                                                             const unsigned *__restrict__ work) {
+   const TileRef r = tile_ref(work, blockIdx.x);
+   const BatchDesc &D = tab[r.inst];
    const Dims d = D.d;
-   const int s0 = __ldg(start + i);
-   norm_final_body(D.rowA, d, D.hx, D.hy, D.state, D.xs, nullptr, blockIdx.x - s0, __ldg(start + i + 1) - s0);
+   norm_final_body(D.rowA, d, D.hx, D.hy, D.state, D.xs, nullptr, r.local,
+                   (d.nx + kNormRowsPerCta - 1) / kNormRowsPerCta);
 }
 
 // ------------------------------------------------------------------- sweeps
@@ -192,7 +193,7 @@ __device__ __forceinline__ void copy_view(SweepView &dst, const SweepView &src) 
 
 template <class R, bool CPLX, int AXIS, bool NU, int MSEG, int S>
 __global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) kb_sweep_xy(const BatchDesc *__restrict__ tab,
-                                                                           const int *__restrict__ start, int n,
+                                                                           const unsigned *__restrict__ work,
                                                                            int ntiles, uint32_t stage_bytes,
                                                                            uint32_t blk_bytes) {
    using P = typename Tr<R, CPLX>::P;
@@ -205,19 +206,22 @@ __global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) kb_sweep_xy(const
    P *blk = (P *) (base + S * stage_bytes);
    double *xtab = (double *) ((unsigned char *) blk + blk_bytes);
    // tile t of the work list: its instance and its place in that instance
+   int acq = -1;  // thread 0: the instance whose tensor maps it last acquired
    auto copy_tile = [&](int t, int q, bool load) {
-      const int i = find_inst(start, n, t);
-      const BatchDesc &D = tab[i];
+      const TileRef r = tile_ref(work, t);
+      const BatchDesc &D = tab[r.inst];
       const SweepView &v = D.sv[AXIS];
       const int TW = v.TW, rows = v.boxn * v.nbox, nzb = (v.d.nz + TW - 1) / TW;
-      const int local = t - __ldg(start + i);
-      const int other = local / nzb, z0 = (local - other * nzb) * TW;
+      const int other = r.local / nzb, z0 = (r.local - other * nzb) * TW;
       P *tile = (P *) (base + q * stage_bytes);
       R *ptile = (R *) (tile + rows * TW);
       const CUtensorMap *tm_psi = &D.tm_psi[AXIS];
-      if (load) {
+      if (r.inst != acq) {
          tmap_acquire(tm_psi);
          if (NU) tmap_acquire(&D.tm_phi);
+         acq = r.inst;
+      }
+      if (load) {
          mbar_arrive_expect_tx(&full[q], (uint32_t) (rows * TW * sizeof(P)) + (NU ? (uint32_t) (rows * TW * sizeof(R)) : 0u));
       }
       for (int b = 0; b < v.nbox; b++) {
@@ -252,7 +256,8 @@ __global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) kb_sweep_xy(const
       }
       // the view and table of this tile's instance (the barrier after the
       // copy wait publishes them)
-      const int i = find_inst(start, n, t);
+      const TileRef r = tile_ref(work, t);
+      const int i = r.inst;
       if (i != cur) {
          // every thread has finished with the previous view and table
          __syncthreads();
@@ -269,8 +274,7 @@ __global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) kb_sweep_xy(const
       const int TW = sv.TW, rows = sv.boxn * sv.nbox, nzb = (sv.d.nz + TW - 1) / TW;
       const int lg = __ffs(TW) - 1;
       const int c = threadIdx.x & (TW - 1), p = threadIdx.x >> lg;
-      const int local = t - __ldg(start + i);
-      const int other = local / nzb, z0 = (local - other * nzb) * TW;
+      const int other = r.local / nzb, z0 = (r.local - other * nzb) * TW;
       P *tile = (P *) (base + q * stage_bytes);
       const double scale = NU ? sv.st->scale : 1.;
       if constexpr (NU && std::is_same<R, double>::value) {
@@ -279,8 +283,9 @@ __global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) kb_sweep_xy(const
          __syncthreads();
       }
       if constexpr (NU && std::is_same<R, float>::value) {
-         const NuTrap<R> xf = nu_reads_fp32<R, AXIS>((const R *) (tile + rows * TW) + c, TW, other, z0, c, sv.d, sv.trap,
-                                                     sv.g, sv.gd, sv.dt, scale);
+         static_assert(AXIS == 0, "calcnu is fused into the x sweep only");
+         const NuTrap32<CPLX> xf = nu_reads_fp32<CPLX>((const float *) (tile + rows * TW) + c, TW, other, z0, c, sv.d,
+                                                       sv.trap, sv.lin, sv.g, sv.gd, sv.dt, scale);
          seg_sweep<R, CPLX, MSEG, 0>(tile, TW, 1, c, p, TW, sv.tb, blk, nullptr, nullptr, nullptr, nullptr, xf);
       } else {
          seg_sweep<R, CPLX, MSEG, 0>(tile, TW, 1, c, p, TW, sv.tb, blk, nullptr, nullptr);
@@ -294,7 +299,7 @@ __global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) kb_sweep_xy(const
 
 template <class R, bool CPLX, int MOM, int MSEG, int S>
 __global__ void __launch_bounds__(256, kSweepCtas[0]) kb_sweep_z(const BatchDesc *__restrict__ tab,
-                                                                 const int *__restrict__ start, int n, int ntiles,
+                                                                 const unsigned *__restrict__ work, int ntiles,
                                                                  uint32_t stage_bytes, uint32_t blk_bytes,
                                                                  uint32_t part_bytes) {
    using P = typename Tr<R, CPLX>::P;
@@ -311,10 +316,10 @@ __global__ void __launch_bounds__(256, kSweepCtas[0]) kb_sweep_z(const BatchDesc
    constexpr bool STAB = std::is_same<R, double>::value;
    constexpr int TE = CPLX ? 2 : 1;
    auto copy_tile = [&](int t, int q, bool load) {
-      const int i = find_inst(start, n, t);
-      const SweepView &v = tab[i].sv[2];
+      const TileRef r = tile_ref(work, t);
+      const SweepView &v = tab[r.inst].sv[2];
       const int TR = v.TW, nz = v.d.nz;
-      const long long r0 = (long long) (t - __ldg(start + i)) * TR;
+      const long long r0 = (long long) r.local * TR;
       const int nr = (int) ((v.d.nxy - r0) < TR ? (v.d.nxy - r0) : TR);
       const uint32_t row_bytes = (uint32_t) (nz * sizeof(P));
       P *tile = (P *) (base + q * stage_bytes);
@@ -340,7 +345,8 @@ __global__ void __launch_bounds__(256, kSweepCtas[0]) kb_sweep_z(const BatchDesc
          wait_stage_free<S>();
          copy_tile(t + gridDim.x, (it + 1) % S, true);
       }
-      const int i = find_inst(start, n, t);
+      const TileRef r = tile_ref(work, t);
+      const int i = r.inst;
       if (i != cur) {
          // every thread has finished with the previous view and tables
          __syncthreads();
@@ -365,7 +371,7 @@ __global__ void __launch_bounds__(256, kSweepCtas[0]) kb_sweep_z(const BatchDesc
       }
       const int TR = sv.TW;
       const int c = threadIdx.x % TR, p = threadIdx.x / TR;
-      const long long r0 = (long long) (t - __ldg(start + i)) * TR;
+      const long long r0 = (long long) r.local * TR;
       const int nr = (int) ((sv.d.nxy - r0) < TR ? (sv.d.nxy - r0) : TR);
       P *tile = (P *) (base + q * stage_bytes);
       zsweep_tile<R, CPLX, MOM, MSEG, 0, STAB>(tile, nr, TR, sv.LS, c, p, tbs, blk, part, part2, sv.wz, sv.wz2, sv.hz3,

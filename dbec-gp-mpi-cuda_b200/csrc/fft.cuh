@@ -10,7 +10,8 @@
 // 128-byte row: bank-conflict free.  This is also the layout a TMA box of L
 // columns by the whole line lands in.
 //
-// Each radix-r stage (autosort Stockham, decimation in time) computes
+// Radices 2, 3, 4, 5, 8 and (FP32, 16 points per thread) 16.  Each radix-r
+// stage (autosort Stockham, decimation in time) computes
 //   j in [0, n/r), k = j mod Ns,  v[t] = src[j + t n/r] * W^(t k n/(Ns r))
 //   v = DFT_r(v),  dst[(j / Ns) Ns r + k + t Ns] = v[t],  Ns *= r
 // leaving the result in natural order; src and dst are the same buffer, the
@@ -103,11 +104,47 @@ template <class C, bool INV> __device__ __forceinline__ void dft8(C *v) {
    v[3] = cadd(e[3], w3);   v[7] = csub(e[3], w3);
 }
 
+// 16-point DFT as 4 x 4 (n = 4 n1 + n2, k = k1 + 4 k2): a DFT4 over n1 for
+// every n2, the twiddles W16^(n2 k1), a DFT4 over n2 for every k1.
+template <class C, bool INV> __device__ __forceinline__ void dft16(C *v) {
+   using R = decltype(v[0].x);
+   const R c1 = (R) 0.92387953251128675613, s1 = (R) 0.38268343236508977173;  // cos, sin(pi / 8)
+   const R h = (R) 0.70710678118654752440;
+   C y[4][4];
+#pragma unroll
+   for (int n2 = 0; n2 < 4; n2++) {
+      C t[4] = {v[n2], v[4 + n2], v[8 + n2], v[12 + n2]};
+      dft4<C, INV>(t);
+#pragma unroll
+      for (int k1 = 0; k1 < 4; k1++) y[n2][k1] = t[k1];
+   }
+   // W16^m, m = n2 k1 in {1, 2, 3, 2, 4, 6, 3, 6, 9} (forward: exp(-2 pi i m / 16))
+   const R sg = INV ? (R) 1 : (R) -1;
+   auto tw = [&](C a, R wr, R wi) -> C { C r; r.x = a.x * wr - a.y * wi; r.y = a.x * wi + a.y * wr; return r; };
+   y[1][1] = tw(y[1][1], c1, sg * s1);
+   y[1][2] = tw(y[1][2], h, sg * h);
+   y[1][3] = tw(y[1][3], s1, sg * c1);
+   y[2][1] = tw(y[2][1], h, sg * h);
+   y[2][2] = mul_mi<C, INV>(y[2][2]);
+   y[2][3] = tw(y[2][3], -h, sg * h);
+   y[3][1] = tw(y[3][1], s1, sg * c1);
+   y[3][2] = tw(y[3][2], -h, sg * h);
+   y[3][3] = tw(y[3][3], -c1, -sg * s1);
+#pragma unroll
+   for (int k1 = 0; k1 < 4; k1++) {
+      C t[4] = {y[0][k1], y[1][k1], y[2][k1], y[3][k1]};
+      dft4<C, INV>(t);
+#pragma unroll
+      for (int k2 = 0; k2 < 4; k2++) v[k1 + 4 * k2] = t[k2];
+   }
+}
+
 template <int R, class C, bool INV> __device__ __forceinline__ void dftr(C *v) {
    if constexpr (R == 2) dft2<C, INV>(v);
    else if constexpr (R == 3) dft3<C, INV>(v);
    else if constexpr (R == 4) dft4<C, INV>(v);
    else if constexpr (R == 5) dft5<C, INV>(v);
+   else if constexpr (R == 16) dft16<C, INV>(v);
    else dft8<C, INV>(v);
 }
 
@@ -166,10 +203,14 @@ __device__ __forceinline__ void fft_stage_ip(C *buf, int n, int Ns, unsigned mag
 // Full in-place transform of L interleaved lines in buf (PPT as above).
 template <int L, class C, bool INV, int PPT>
 __device__ __forceinline__ void fft_lines_ip(C *buf, const FftPlan &pl, const C *tw, int twmul) {
-   // make_plan orders the stages by radix (8, 4, 2, 3, 5): one loop per radix
-   // (a switch over the radix inside one loop made ptxas spill the values
-   // held across the barriers)
+   // make_plan orders the stages by radix (16, 8, 4, 2, 3, 5): one loop per
+   // radix (a switch over the radix inside one loop made ptxas spill the
+   // values held across the barriers).  Radix 16 only where a thread holds
+   // 16 points (PPT >= 16, the FP32 passes).
    int st = 0;
+   if constexpr (PPT >= 16)
+      for (; st < pl.nst && pl.rad[st] == 16; st++)
+         fft_stage_ip<16, L, C, INV, PPT>(buf, pl.n, pl.ns[st], pl.magic[st], tw, twmul);
    for (; st < pl.nst && pl.rad[st] == 8; st++) fft_stage_ip<8, L, C, INV, PPT>(buf, pl.n, pl.ns[st], pl.magic[st], tw, twmul);
    for (; st < pl.nst && pl.rad[st] == 4; st++) fft_stage_ip<4, L, C, INV, PPT>(buf, pl.n, pl.ns[st], pl.magic[st], tw, twmul);
    for (; st < pl.nst && pl.rad[st] == 2; st++) fft_stage_ip<2, L, C, INV, PPT>(buf, pl.n, pl.ns[st], pl.magic[st], tw, twmul);

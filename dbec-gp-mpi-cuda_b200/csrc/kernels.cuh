@@ -45,6 +45,7 @@ __device__ __forceinline__ float arn(float a, float b) { return __fadd_rn(a, b);
 // (imag3d-mpicuda.cu:872-889): 0.5 * par * (g2 x^2 + n2 y^2 + l2 z^2).
 struct Trap {
    const double *x2, *y2, *z2;
+   const float *x2f, *y2f, *z2f;  // FP32 copies (mixed precision)
    double hp;  // 0.5 * par
    double vg2, vn2, vl2;
    __device__ __forceinline__ double v(int i, int j, int k) const {
@@ -57,6 +58,7 @@ struct Trap {
 // n2 y^2 + l2 z^2) is a sum over the axes, so exp(-dt V) is a product of one
 // factor per axis; the factors are tabulated per axis on the host (long
 // double) and only the nonlinear part of the exponent is evaluated per point.
+// The tables are FP64 for FP64 handles and FP32 for mixed-precision ones.
 struct LinPhase {
    const void *ex, *ey, *ez;
 };

@@ -82,6 +82,7 @@ struct gpe_solver {
    void *alpha[3] = {nullptr, nullptr, nullptr}, *gamma[3] = {nullptr, nullptr, nullptr};
    double2 A[3], A0r[3], mA[3];
    double *x2 = nullptr, *y2 = nullptr, *z2 = nullptr;
+   float *x2f = nullptr, *y2f = nullptr, *z2f = nullptr;  // FP32 copies (mixed precision)
    void *lin[3] = {nullptr, nullptr, nullptr};  // per-axis trap factors of calcnu, imag (LinPhase)
    double *rowA = nullptr, *rowB = nullptr, *tmp = nullptr, *obs = nullptr;
    double *rms_buf = nullptr;  // rms samples of gpe_run, kRmsSlots x 4 doubles
@@ -98,6 +99,9 @@ struct gpe_solver {
       CUtensorMap tm_psi{}, tm_phi{};
       SegTab tab{};
       void *M = nullptr, *N = nullptr;
+      // mixed precision: alpha, gamma, M, N rounded once to FP32 (the values
+      // the FP32 sweeps would otherwise round from the FP64 tables at every use)
+      void *t32[4] = {nullptr, nullptr, nullptr, nullptr};
    } sw[3];
    double *wz = nullptr;      // Simpson weights along z (norm partials)
    double *wz2 = nullptr;     // wz[k] * z[k]^2 (rms partials)
@@ -119,14 +123,15 @@ static void mark(gpe_solver *s) {
 
 // ---------------------------------------------------------------- planning
 // Radices in the order the stages are grouped (fft_lines_ip loops over them
-// in this order); max_radix 4 or 2 drops the larger powers of two.
+// in this order); max_radix 8, 4 or 2 drops the larger powers of two.  Radix
+// 16 is for the FP32 passes only, whose threads hold 16 points.
 static bool make_plan(int n, FftPlan &pl, int max_radix = 8) {
    pl.n = n;
    pl.nst = 0;
    int m = n;
-   static const int pref[] = {8, 4, 2, 3, 5};
+   static const int pref[] = {16, 8, 4, 2, 3, 5};
    for (int r : pref) {
-      if ((r == 8 || r == 4) && r > max_radix) continue;
+      if ((r == 16 || r == 8 || r == 4) && r > max_radix) continue;
       while (m % r == 0 && pl.nst < kMaxStages) { pl.rad[pl.nst++] = r; m /= r; }
    }
    int ns = 1;
@@ -294,6 +299,25 @@ static gpe_status make_segtab(gpe_solver *s, int ax, long n, double d2, int m, i
    t.ga = s->gamma[ax];
    t.M = s->sw[ax].M;
    t.N = s->sw[ax].N;
+   if (s->fp32) {
+      // FP32 copies of the FP64 tables (alpha and gamma stay FP64 in HBM as
+      // computed; the FP32 kernels read these once-rounded copies)
+      const void *src[4] = {s->alpha[ax], s->gamma[ax], s->sw[ax].M, s->sw[ax].N};
+      const size_t nd = (size_t) n * (s->cplx ? 2 : 1);
+      std::vector<double> h(nd);
+      std::vector<float> f(nd);
+      for (int q = 0; q < 4; q++) {
+         if (s->sw[ax].t32[q]) cudaFree(s->sw[ax].t32[q]);
+         s->sw[ax].t32[q] = nullptr;
+         CK(cudaMemcpy(h.data(), src[q], sizeof(double) * nd, cudaMemcpyDeviceToHost));
+         for (size_t e = 0; e < nd; e++) f[e] = (float) h[e];
+         CKS(upload(&s->sw[ax].t32[q], f.data(), nd));
+      }
+      t.al = s->sw[ax].t32[0];
+      t.ga = s->sw[ax].t32[1];
+      t.M = s->sw[ax].t32[2];
+      t.N = s->sw[ax].t32[3];
+   }
    t.A = s->A[ax];
    t.A0r = s->A0r[ax];
    t.mA = s->mA[ax];
@@ -472,8 +496,12 @@ static gpe_status plan_tiles(gpe_solver *s) {
                                        "at most 256 PPT points per tile");
          *Ls[a] = L;
       }
-      const int mr = s->tune.fft_max_radix > 0 ? s->tune.fft_max_radix : 8;
-      if (mr != 8 && mr != 4 && mr != 2) return fail(GPE_ERR_PARAM, "tuning: fft_max_radix must be 8, 4 or 2");
+      // FP32 passes hold 16 points per thread and default to radix-16 stages
+      // (two stages instead of three for 128- and 256-point lines)
+      const int mr = s->tune.fft_max_radix > 0 ? s->tune.fft_max_radix : (s->fp32 ? 16 : 8);
+      if (mr != 16 && mr != 8 && mr != 4 && mr != 2)
+         return fail(GPE_ERR_PARAM, "tuning: fft_max_radix must be 16, 8, 4 or 2");
+      if (mr == 16 && !s->fp32) return fail(GPE_ERR_PARAM, "tuning: radix 16 is for mixed precision only");
       make_plan(d.nx, s->px, mr);
       make_plan(d.ny, s->py, mr);
       make_plan(d.nz / 2, s->ph, mr);
@@ -536,7 +564,7 @@ static gpe_status make_udd(gpe_solver *s) {
 }
 
 static void free_all(gpe_solver *s) {
-   void *ptrs[] = {s->psi, s->spec, s->phi, s->twx, s->twy, s->twz, s->udd, s->x2, s->y2, s->z2,
+   void *ptrs[] = {s->psi, s->spec, s->phi, s->twx, s->twy, s->twz, s->udd, s->x2, s->y2, s->z2, s->x2f, s->y2f, s->z2f,
                    s->rowA, s->rowB, s->tmp, s->obs, s->state, s->rms_buf};
    for (void *q : ptrs)
       if (q) cudaFree(q);
@@ -545,6 +573,8 @@ static void free_all(gpe_solver *s) {
       if (s->gamma[a]) cudaFree(s->gamma[a]);
       if (s->sw[a].M) cudaFree(s->sw[a].M);
       if (s->sw[a].N) cudaFree(s->sw[a].N);
+      for (void *q : s->sw[a].t32)
+         if (q) cudaFree(q);
    }
    if (s->wz) cudaFree(s->wz);
    for (void *q : s->lin)
@@ -617,6 +647,15 @@ static gpe_status create_impl(const gpe_params *p, void *stream, gpe_solver *s) 
    CKS(upload(&t, s->hx2.data(), d.nx)); s->x2 = (double *) t;
    CKS(upload(&t, s->hy2.data(), d.ny)); s->y2 = (double *) t;
    CKS(upload(&t, s->hz2.data(), d.nz)); s->z2 = (double *) t;
+   if (s->fp32) {
+      const std::vector<double> *sq[3] = {&s->hx2, &s->hy2, &s->hz2};
+      float **dst[3] = {&s->x2f, &s->y2f, &s->z2f};
+      for (int a = 0; a < 3; a++) {
+         std::vector<float> f(sq[a]->begin(), sq[a]->end());
+         CKS(upload(&t, f.data(), f.size()));
+         *dst[a] = (float *) t;
+      }
+   }
    // trap factors per axis for calcnu in imaginary time: exp(-dt 0.5 par c x^2)
    if (!s->cplx) {
       const long double hp = 0.5L * (long double) s->par, dt = (long double) p->dt;
@@ -627,7 +666,12 @@ static gpe_status create_impl(const gpe_params *p, void *stream, gpe_solver *s) 
          const size_t n = sq[a]->size();
          std::vector<double> tab(n);
          for (size_t i = 0; i < n; i++) tab[i] = (double) expl(-dt * hp * cf[a] * (long double) (*sq[a])[i]);
-         CKS(upload(&s->lin[a], tab.data(), tab.size()));
+         if (s->fp32) {
+            std::vector<float> f(tab.begin(), tab.end());
+            CKS(upload(&s->lin[a], f.data(), f.size()));
+         } else {
+            CKS(upload(&s->lin[a], tab.data(), tab.size()));
+         }
       }
    }
    CK(cudaDeviceSynchronize());
@@ -664,6 +708,7 @@ extern "C" const char *gpe_last_error(void) { return g_err.c_str(); }
 static Trap trap_of(const gpe_solver *s) {
    Trap t;
    t.x2 = s->x2; t.y2 = s->y2; t.z2 = s->z2;
+   t.x2f = s->x2f; t.y2f = s->y2f; t.z2f = s->z2f;
    t.hp = 0.5 * s->par;
    t.vg2 = s->p.gamma * s->p.gamma;
    t.vn2 = s->p.nu * s->p.nu;
@@ -717,8 +762,12 @@ template <class R, bool CPLX> struct Impl {
       if (ppt <= 16) return f(std::integral_constant<int, 16>());
       return f(std::integral_constant<int, 32>());
    }
-   // points per thread of the z passes: (nz/2) L over 256 threads
-   static int zppt(const gpe_solver *s, int L) { return (int) (((s->d.nz / 2) * L + 255) / 256); }
+   // points per thread of the z passes: (nz/2) L over 256 threads, at least
+   // 16 in FP32 (the radix-16 stages need them)
+   static int zppt(const gpe_solver *s, int L) {
+      const int p = (int) (((s->d.nz / 2) * L + 255) / 256);
+      return s->fp32 ? std::max(p, 16) : p;
+   }
    // threads of a z inverse pass CTA, and of a forward pass CTA over real
    // rows: PPT points each of the L half-length lines (the forward passes
    // over complex rows keep 256: sized CTAs measured slower there, 101 -> 105
@@ -1649,7 +1698,7 @@ extern "C" gpe_status gpe_get_tuning(gpe_solver *s, gpe_tuning *t) {
    }
    t->fft_tile[0] = s->Ly;
    t->fft_tile[1] = s->Lx;
-   t->fft_max_radix = s->tune.fft_max_radix > 0 ? s->tune.fft_max_radix : 8;
+   t->fft_max_radix = s->tune.fft_max_radix > 0 ? s->tune.fft_max_radix : (s->fp32 ? 16 : 8);
    return GPE_OK;
 }
 
@@ -1737,7 +1786,7 @@ extern "C" gpe_status gpe_autotune(gpe_solver *s, double g, double gd, int nstep
       if (ms[1] + ms[3] < best_y) { best_y = ms[1] + ms[3]; pick.fft_tile[0] = L; }
       if (ms[2] < best_x) { best_x = ms[2]; pick.fft_tile[1] = L; }
    }
-   for (int r = 8; r >= 2 && st == GPE_OK; r /= 2) {
+   for (int r = s->fp32 ? 16 : 8; r >= 2 && st == GPE_OK; r /= 2) {
       gpe_tuning t = pick;
       t.fft_max_radix = r;
       s->tune = t;

@@ -27,7 +27,8 @@ namespace gpe {
 
 // Segment tables of one axis.
 struct SegTab {
-   const void *al, *ga;  // alpha, gamma padded to n entries (double or double2)
+   const void *al, *ga;  // alpha, gamma padded to n entries (double or double2;
+                         // float or float2 for the FP32 sweeps)
    const void *M, *N;    // prefix products, n entries each
    double2 A, A0r, mA;
    int n, m, P;
@@ -35,8 +36,13 @@ struct SegTab {
 
 template <class R, bool CPLX> struct SegOps {
    using P = typename Tr<R, CPLX>::P;
+   // table entry i: FP64 tables for FP64 sweeps, their once-rounded FP32
+   // copies for FP32 sweeps
    __device__ static P ld(const void *t, int i) {
-      if constexpr (CPLX) {
+      if constexpr (std::is_same<R, float>::value) {
+         if constexpr (CPLX) return __ldg((const float2 *) t + i);
+         else return __ldg((const float *) t + i);
+      } else if constexpr (CPLX) {
          const double2 v = __ldg((const double2 *) t + i);
          return mk<R>((R) v.x, (R) v.y);
       } else {
@@ -249,23 +255,6 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
    if (simp2) *simp2 = acc2;
 }
 
-// calcnu fused into the x sweep's reads (calcnu_kernel imag3d-mpicuda.cu:1759,
-// real3d-mpicuda.cu:1856): element i of column c of the tile, with the
-// pending 1/norm applied first; V is recomputed from the trap tables (the
-// terms of the two fixed coordinates hoisted per column).
-template <class R> struct NuTrap {
-   const R *ptile;  // phi tile, row stride tw
-   int tw;
-   const double *va;
-   double ca, to, tz, hp, scale;
-   R g, gd, dt, invN;
-   template <class P> __device__ __forceinline__ P operator()(P v, int i) const {
-      const double sv = arn(arn(mrn(ca, va[i]), to), tz);
-      const R V = (R) mrn(hp, sv);
-      return nu_op<R>(scl(v, scale), ptile[i * tw], V, g, gd, dt, invN);
-   }
-};
-
 // FP64 calcnu over a staged tile before its sweep (the x sweep's fused
 // calcnu_kernel, imag3d-mpicuda.cu:1759, real3d-mpicuda.cu:1856), one z
 // column per thread, with the pending 1/norm applied first.  Tile t of the
@@ -308,18 +297,63 @@ __device__ __forceinline__ void nu_pass_fp64(typename Tr<R, CPLX>::P *tile, cons
    }
 }
 
-// FP32: calcnu applied as the sweep's recurrence reads each point (measured
-// faster than the separate pass over the tile; slower in FP64, where a
-// thread's extra evaluations for the two points above its segment cost more).
-template <class R, int AXIS>
-__device__ __forceinline__ NuTrap<R> nu_reads_fp32(const R *ptile_c, int TW, int other, int z0, int c, const Dims &d,
-                                                   const Trap &trap, double g, double gd, double dt, double scale) {
-   const R invN = (R) (1.0 / (double) d.npts);
+// calcnu of the mixed-precision x sweep, applied as the sweep's recurrence
+// reads each point (measured faster than a separate pass over the tile in
+// FP32; slower in FP64, where a thread's extra evaluations for the two points
+// above its segment cost more), entirely in FP32 like the step's other
+// exponentials: real time recomputes V from the FP32 trap tables (the order
+// of Trap::v) and takes sincosf of the exponent; imaginary time multiplies the
+// FP32 trap factors exp(-dt V_x) exp(-dt V_y) exp(-dt V_z) and takes expf of
+// the nonlinear part only.  The pending 1/norm is applied first.
+template <bool CPLX> struct NuTrap32 {
+   const float *ptile;  // phi tile, row stride tw
+   int tw;
+   const float *va;     // along the line: x^2 (real time) or exp(-dt V_x) (imaginary time)
+   float ca, to, tz, hp;  // real time: V = hp ((ca va + to) + tz)
+   float lfix;            // imaginary time: exp(-dt V_y) exp(-dt V_z) of this column
+   float scale, g, gd, dt, invN;
+   template <class P> __device__ __forceinline__ P operator()(P v, int i) const {
+      const float phi = ptile[i * tw];
+      if constexpr (CPLX) {
+         const float2 p = make_float2(v.x * scale, v.y * scale);
+         const float sv = __fadd_rn(__fadd_rn(__fmul_rn(ca, va[i]), to), tz);
+         return nu_op<float>(p, phi, __fmul_rn(hp, sv), g, gd, dt, invN);
+      } else {
+         const float p = v * scale;
+         const float thn = dt * fmaf(p * p, g, (phi * invN) * gd);
+         return p * ((va[i] * lfix) * expf(-thn));
+      }
+   }
+};
+
+// The calcnu functor of tile column c of an x sweep tile covering z columns
+// [z0, z0 + TW) of plane y = other (mixed precision).
+template <bool CPLX>
+__device__ __forceinline__ NuTrap32<CPLX> nu_reads_fp32(const float *ptile_c, int TW, int other, int z0, int c,
+                                                        const Dims &d, const Trap &trap, const LinPhase &lin, double g,
+                                                        double gd, double dt, double scale) {
    const int k = min(z0 + c, d.nz - 1);  // columns past nz are zero fill, never stored
-   const double tz = mrn(trap.vl2, trap.z2[k]);
-   const double to = AXIS == 0 ? mrn(trap.vn2, trap.y2[other]) : mrn(trap.vg2, trap.x2[other]);
-   return NuTrap<R>{ptile_c, TW, AXIS == 0 ? trap.x2 : trap.y2, AXIS == 0 ? trap.vg2 : trap.vn2, to, tz, trap.hp, scale,
-                    (R) g, (R) gd, (R) dt, invN};
+   NuTrap32<CPLX> f;
+   f.ptile = ptile_c;
+   f.tw = TW;
+   f.scale = (float) scale;
+   f.g = (float) g;
+   f.gd = (float) gd;
+   f.dt = (float) dt;
+   f.invN = (float) (1.0 / (double) d.npts);
+   if constexpr (CPLX) {
+      f.va = trap.x2f;
+      f.ca = (float) trap.vg2;
+      f.to = __fmul_rn((float) trap.vn2, trap.y2f[other]);
+      f.tz = __fmul_rn((float) trap.vl2, trap.z2f[k]);
+      f.hp = (float) trap.hp;
+      f.lfix = 0.f;
+   } else {
+      f.va = (const float *) lin.ex;
+      f.lfix = __ldg((const float *) lin.ey + other) * __ldg((const float *) lin.ez + k);
+      f.ca = f.to = f.tz = f.hp = 0.f;
+   }
+   return f;
 }
 
 // ---------------------------------------------------------------------------
@@ -424,8 +458,9 @@ __global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) k_sweep_xy(const 
          __syncthreads();
       }
       if constexpr (NU && std::is_same<R, float>::value) {
-         const NuTrap<R> xf = nu_reads_fp32<R, AXIS>((const R *) (tile + rows * TW) + c, TW, other, z0, c, d, trap, g,
-                                                     gd, dt, scale);
+         static_assert(AXIS == 0, "calcnu is fused into the x sweep only");
+         const NuTrap32<CPLX> xf = nu_reads_fp32<CPLX>((const float *) (tile + rows * TW) + c, TW, other, z0, c, d,
+                                                       trap, lin, g, gd, dt, scale);
          seg_sweep<R, CPLX, MSEG, TWC>(tile, TW, 1, c, p, TW, tb, blk, nullptr, nullptr, nullptr, nullptr, xf);
       } else {
          seg_sweep<R, CPLX, MSEG, TWC>(tile, TW, 1, c, p, TW, tb, blk, nullptr, nullptr);

@@ -107,6 +107,7 @@ _SIGS = {
     "gpe_batch_autotune": (C.c_int, [_P, C.c_int]),
     "gpe_batch_run": (C.c_int, [_P, C.c_long]),
     "gpe_batch_time_steps": (C.c_int, [_P, C.c_long, _DP]),
+    "gpe_batch_profile_step": (C.c_int, [_P, C.c_long, _P, C.c_int, C.POINTER(C.c_int)]),
     "gpe_batch_launch_count": (C.c_int, [_P, C.POINTER(C.c_longlong)]),
     "gpe_server_create": (C.c_int, [C.c_int, C.c_longlong, C.c_int, C.POINTER(_P)]),
     "gpe_server_destroy": (None, [_P]),
@@ -419,6 +420,16 @@ class Batch:
         ms = C.c_double()
         _check(lib().gpe_batch_time_steps(self.h, int(nsteps), C.byref(ms)))
         return ms.value
+
+    BATCH_PASSES = ("zfwd_r2c", "yfft_fwd", "xconv_udd", "yfft_inv", "zinv_c2r", "phi_boundary", "xsweep_calcnu",
+                    "ysweep", "zsweep", "norm_final")
+
+    def profile_step(self, nsteps):
+        """Mean milliseconds per batch step of every pass: [(name, ms)]."""
+        ms = np.zeros(16)
+        n = C.c_int()
+        _check(lib().gpe_batch_profile_step(self.h, int(nsteps), _ptr(ms), 16, C.byref(n)))
+        return [(self.BATCH_PASSES[i], float(ms[i])) for i in range(n.value)]
 
     def launch_count(self):
         v = C.c_longlong()

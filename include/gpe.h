@@ -155,7 +155,7 @@ typedef struct gpe_tuning {
    int sweep_tw[3];     /* lines per CTA of the x, y, z sweeps (a power of two) */
    int sweep_stages[3]; /* TMA pipeline depth of the x, y, z sweeps: 2 or 3 */
    int fft_tile[2];     /* kz columns per tile of the y and x FFT passes */
-   int fft_max_radix;   /* largest radix of the FFT plans: 8, 4 or 2 */
+   int fft_max_radix;   /* largest radix of the FFT plans: 16 (mixed precision only), 8, 4 or 2 */
 } gpe_tuning;
 /* The configuration in use (every field filled in). */
 gpe_status gpe_get_tuning(gpe_solver *s, gpe_tuning *t);
@@ -206,6 +206,12 @@ gpe_status gpe_batch_autotune(gpe_batch *b, int nsteps);
 gpe_status gpe_batch_run(gpe_batch *b, long nsteps);
 /* nsteps batch steps bracketed by CUDA events: elapsed milliseconds. */
 gpe_status gpe_batch_time_steps(gpe_batch *b, long nsteps, double *ms);
+/* Per-pass timing of batch steps: nsteps steps launched pass by pass with a
+ * CUDA event after every pass; ms[q] (q < *count = 10, cap >= 10) receives the
+ * mean milliseconds of pass q per step, summed over the groups, in the order
+ * z forward FFT, y FFT, x convolution, inverse y FFT, z inverse FFT, phi
+ * boundary planes, x sweep with calcnu, y sweep, z sweep, norm. */
+gpe_status gpe_batch_profile_step(gpe_batch *b, long nsteps, double *ms, int cap, int *count);
 /* Kernel launches executed by batch steps so far. */
 gpe_status gpe_batch_launch_count(gpe_batch *b, long long *count);
 
