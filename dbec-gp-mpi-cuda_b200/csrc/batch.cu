@@ -38,9 +38,7 @@ struct Group {
    long long off[kNPass + 1] = {};  // start of each pass's work list in dwork
    BatchDesc *dtab = nullptr;        // device descriptor table
    unsigned *dwork = nullptr;        // device work lists (TileRef packed per tile)
-   int *drange = nullptr;            // device: per sweep, the CTAs' ranges of its work list
    int sweep_grid[3] = {0, 0, 0};
-   int range_off[3] = {0, 0, 0};  // start of each sweep's CTA ranges in drange
    size_t sweep_smem[3] = {0, 0, 0};
 };
 
@@ -91,7 +89,6 @@ void drop_tables(gpe_batch *b) {
    for (Group &G : b->groups) {
       if (G.dtab) cudaFree(G.dtab);
       if (G.dwork) cudaFree(G.dwork);
-      if (G.drange) cudaFree(G.drange);
    }
    b->groups.clear();
    b->tables = false;
@@ -181,32 +178,8 @@ gpe_status build_tables(gpe_batch *b) {
          for (int k = 0; k < n; k++)
             for (long long t = 0; t < geo[k].tiles[q]; t++) work[e++] = ((unsigned) k << kLocalBits) | (unsigned) t;
       }
-      // sweep CTAs: contiguous ranges of the work list with about equal
-      // numbers of grid points
-      std::vector<int> range;
-      for (int a = 0; a < 3; a++) {
-         const int grid = G.sweep_grid[a];
-         long long total = 0;
-         for (int k = 0; k < n; k++) total += geo[k].tiles[kPXsweep + a] * geo[k].tile_pts[a];
-         const size_t r0 = range.size();
-         range.push_back(0);
-         long long cum = 0;
-         int t = 0, cta = 1;
-         for (int k = 0; k < n; k++)
-            for (long long j = 0; j < geo[k].tiles[kPXsweep + a]; j++, t++) {
-               cum += geo[k].tile_pts[a];
-               while (cta < grid && cum * grid >= total * cta) {
-                  range.push_back(t + 1);
-                  cta++;
-               }
-            }
-         while ((int) (range.size() - r0) < grid + 1) range.push_back(t);
-         G.range_off[a] = (int) r0;
-      }
       std::vector<BatchDesc> h;
       BCKS(group_descs(b, G, h));
-      BCK(cudaMalloc(&G.drange, sizeof(int) * range.size()));
-      BCK(cudaMemcpyAsync(G.drange, range.data(), sizeof(int) * range.size(), cudaMemcpyHostToDevice, b->master));
       BCK(cudaMalloc(&G.dtab, sizeof(BatchDesc) * h.size()));
       BCK(cudaMalloc(&G.dwork, sizeof(unsigned) * std::max<size_t>(1, work.size())));
       BCK(cudaMemcpyAsync(G.dtab, h.data(), sizeof(BatchDesc) * h.size(), cudaMemcpyHostToDevice, b->master));
@@ -289,20 +262,20 @@ template <class R, bool CPLX> struct BatchStep {
       BCKS(with_mseg(A.mseg[0], [&](auto mc) {
          constexpr int M = decltype(mc)::value;
          return launch(kb_sweep_xy<R, CPLX, 0, true, M, 2>, (unsigned) G.sweep_grid[0], A.threads[kPXsweep],
-                       G.sweep_smem[0], st, tab, S(kPXsweep), G.drange + G.range_off[0], A.stage[0], A.blk[0]);
+                       G.sweep_smem[0], st, tab, S(kPXsweep), (int) A.tiles[kPXsweep], A.stage[0], A.blk[0]);
       }));
       BCKS(mark(kPXsweep));
       BCKS(with_mseg(A.mseg[1], [&](auto mc) {
          constexpr int M = decltype(mc)::value;
          return launch(kb_sweep_xy<R, CPLX, 1, false, M, 2>, (unsigned) G.sweep_grid[1], A.threads[kPYsweep],
-                       G.sweep_smem[1], st, tab, S(kPYsweep), G.drange + G.range_off[1], A.stage[1], A.blk[1]);
+                       G.sweep_smem[1], st, tab, S(kPYsweep), (int) A.tiles[kPYsweep], A.stage[1], A.blk[1]);
       }));
       BCKS(mark(kPYsweep));
       BCKS(with_mseg(A.mseg[2], [&](auto mc) {
          constexpr int M = decltype(mc)::value;
          constexpr int MOM = CPLX ? 0 : 1;
          return launch(kb_sweep_z<R, CPLX, MOM, M, 2>, (unsigned) G.sweep_grid[2], A.threads[kPZsweep],
-                       G.sweep_smem[2], st, tab, S(kPZsweep), G.drange + G.range_off[2], A.stage[2], A.blk[2],
+                       G.sweep_smem[2], st, tab, S(kPZsweep), (int) A.tiles[kPZsweep], A.stage[2], A.blk[2],
                        A.part);
       }));
       BCKS(mark(kPZsweep));

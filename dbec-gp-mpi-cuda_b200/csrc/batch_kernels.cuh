@@ -74,7 +74,6 @@ struct BatchGeom {
    uint32_t blk[3];          // sweeps: bytes of the block maps
    uint32_t extra[3];        // sweeps: FP64 tables (x: calcnu table; z: coefficient tables)
    uint32_t part;            // z sweep: bytes of one Simpson partial array
-   long long tile_pts[3];    // sweeps: grid points of one tile (the work balance of the ranges)
    int Ly, Lx;               // the instance's own FFT tile widths
 };
 
@@ -178,13 +177,12 @@ static __global__ void __launch_bounds__(32 * kNormRowsPerCta) kb_norm_final(con
 
 // ------------------------------------------------------------------- sweeps
 // Persistent pipelined CTAs over the tiles of all instances (the pipeline of
-// k_sweep_xy / k_sweep_z): each CTA walks a contiguous range of the work
-// list (range[b] .. range[b + 1], balanced by tile size on the host), and
-// while it sweeps tile t, tile t + 1 (possibly of the next instance) is
-// loading.  Every stage has room for the largest tile of the group
-// (stage_bytes); the view of the tile's instance is copied into shared
-// memory when the instance changes, and so are the FP64 tables the
-// single-solve kernels stage once per CTA.
+// k_sweep_xy / k_sweep_z): while a CTA sweeps tile t, tile t + gridDim.x
+// (possibly of another instance) is loading.  Every stage has room for the
+// largest tile of the group (stage_bytes); the view of the tile's instance
+// is copied into shared memory when the instance changes from one tile of
+// the CTA to the next, and so are the FP64 tables the single-solve kernels
+// stage once per CTA.
 
 // Words of a view copied by the CTA (every thread calls it).
 __device__ __forceinline__ void copy_view(SweepView &dst, const SweepView &src) {
@@ -196,8 +194,8 @@ __device__ __forceinline__ void copy_view(SweepView &dst, const SweepView &src) 
 template <class R, bool CPLX, int AXIS, bool NU, int MSEG, int S>
 __global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) kb_sweep_xy(const BatchDesc *__restrict__ tab,
                                                                            const unsigned *__restrict__ work,
-                                                                           const int *__restrict__ range,
-                                                                           uint32_t stage_bytes, uint32_t blk_bytes) {
+                                                                           int ntiles, uint32_t stage_bytes,
+                                                                           uint32_t blk_bytes) {
    using P = typename Tr<R, CPLX>::P;
    extern __shared__ __align__(16) unsigned char smem_raw[];
    __shared__ __align__(8) uint64_t full[S];
@@ -247,17 +245,14 @@ __global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) kb_sweep_xy(const
       fence_mbar_init();
    }
    __syncthreads();
-   // this CTA's contiguous range of the work list (balanced by tile size on
-   // the host), so that it moves to another instance rarely
-   const int t0 = __ldg(range + blockIdx.x), t1 = __ldg(range + blockIdx.x + 1);
-   if (threadIdx.x == 0 && t0 < t1) copy_tile(t0, 0, true);
+   if (threadIdx.x == 0 && (int) blockIdx.x < ntiles) copy_tile(blockIdx.x, 0, true);
    int cur = -1;  // instance whose view is in sv
    int it = 0;
-   for (int t = t0; t < t1; t++, it++) {
+   for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
       const int q = it % S;
-      if (threadIdx.x == 0 && t + 1 < t1) {
+      if (threadIdx.x == 0 && t + (int) gridDim.x < ntiles) {
          wait_stage_free<S>();
-         copy_tile(t + 1, (it + 1) % S, true);
+         copy_tile(t + gridDim.x, (it + 1) % S, true);
       }
       // the view and table of this tile's instance (the barrier after the
       // copy wait publishes them)
@@ -304,8 +299,7 @@ __global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) kb_sweep_xy(const
 
 template <class R, bool CPLX, int MOM, int MSEG, int S>
 __global__ void __launch_bounds__(256, kSweepCtas[0]) kb_sweep_z(const BatchDesc *__restrict__ tab,
-                                                                 const unsigned *__restrict__ work,
-                                                                 const int *__restrict__ range,
+                                                                 const unsigned *__restrict__ work, int ntiles,
                                                                  uint32_t stage_bytes, uint32_t blk_bytes,
                                                                  uint32_t part_bytes) {
    using P = typename Tr<R, CPLX>::P;
@@ -321,8 +315,9 @@ __global__ void __launch_bounds__(256, kSweepCtas[0]) kb_sweep_z(const BatchDesc
    // FP64: the coefficient tables staged in shared memory, as k_sweep_z does
    constexpr bool STAB = std::is_same<R, double>::value;
    constexpr int TE = CPLX ? 2 : 1;
-   // one bulk copy per row, issued by the 32 lanes of warp 0; every lane
-   // commits and waits for its own store groups
+   // one bulk copy per row, issued by the 32 lanes of warp 0 (the short rows
+   // of small grids make many small copies); every lane commits and waits
+   // for its own store groups
    const int lane = threadIdx.x & 31;
    auto copy_tile = [&](int t, int q, bool load) {
       const TileRef r = tile_ref(work, t);
@@ -346,15 +341,14 @@ __global__ void __launch_bounds__(256, kSweepCtas[0]) kb_sweep_z(const BatchDesc
       fence_mbar_init();
    }
    __syncthreads();
-   const int t0 = __ldg(range + blockIdx.x), t1 = __ldg(range + blockIdx.x + 1);
-   if (threadIdx.x < 32 && t0 < t1) copy_tile(t0, 0, true);
+   if (threadIdx.x < 32 && (int) blockIdx.x < ntiles) copy_tile(blockIdx.x, 0, true);
    int cur = -1;
    int it = 0;
-   for (int t = t0; t < t1; t++, it++) {
+   for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
       const int q = it % S;
-      if (threadIdx.x < 32 && t + 1 < t1) {
+      if (threadIdx.x < 32 && t + (int) gridDim.x < ntiles) {
          wait_stage_free<S>();
-         copy_tile(t + 1, (it + 1) % S, true);
+         copy_tile(t + gridDim.x, (it + 1) % S, true);
       }
       const TileRef r = tile_ref(work, t);
       const int i = r.inst;

@@ -1103,7 +1103,6 @@ template <class R, bool CPLX> struct Impl {
          g->threads[kp] = (unsigned) ((TW * P + 31) & ~31);
          const int nzb = (d.nz + TW - 1) / TW;
          g->tiles[kp] = ax == 0 ? (long long) d.ny * nzb : (ax == 1 ? (long long) d.nx * nzb : (d.nxy + TW - 1) / TW);
-         g->tile_pts[ax] = (long long) TW * (ax == 0 ? d.nx : (ax == 1 ? d.ny : d.nz));
          size_t stage;
          if (ax < 2) {
             const size_t rows = (size_t) w.boxn * w.nbox;

@@ -555,16 +555,11 @@ __global__ void __launch_bounds__(256, kSweepCtas[0]) k_sweep_z(typename Tr<R, C
       const long long r0 = (long long) t * TR;
       return (int) ((d.nxy - r0) < TR ? (d.nxy - r0) : TR);
    };
-   // one bulk copy per row, issued by the 32 lanes of warp 0 (a tile of short
-   // rows is many small copies); every lane commits and waits for its own
-   // store groups
-   const int lane = threadIdx.x & 31;
    auto copy_tile = [&](int t, int q, bool load) {
       P *tile = (P *) (base + q * stage_bytes);
       const int nr = nrows(t);
-      if (load && lane == 0) mbar_arrive_expect_tx(&full[q], row_bytes * nr);
-      __syncwarp();
-      for (int r = lane; r < nr; r += 32) {
+      if (load) mbar_arrive_expect_tx(&full[q], row_bytes * nr);
+      for (int r = 0; r < nr; r++) {
          P *g = psi + ((long long) t * TR + r) * nz;
          if (load) bulk_load(tile + r * LS, g, row_bytes, &full[q]);
          else bulk_store(g, tile + r * LS, row_bytes);
@@ -576,12 +571,12 @@ __global__ void __launch_bounds__(256, kSweepCtas[0]) k_sweep_z(typename Tr<R, C
       fence_mbar_init();
    }
    __syncthreads();
-   if (threadIdx.x < 32 && (int) blockIdx.x < ntiles) copy_tile(blockIdx.x, 0, true);
+   if (threadIdx.x == 0 && (int) blockIdx.x < ntiles) copy_tile(blockIdx.x, 0, true);
    const int c = threadIdx.x % TR, p = threadIdx.x / TR;
    int i = 0;
    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, i++) {
       const int q = i % S;
-      if (threadIdx.x < 32 && t + (int) gridDim.x < ntiles) {
+      if (threadIdx.x == 0 && t + (int) gridDim.x < ntiles) {
          wait_stage_free<S>();
          copy_tile(t + gridDim.x, (i + 1) % S, true);
       }
@@ -589,9 +584,9 @@ __global__ void __launch_bounds__(256, kSweepCtas[0]) k_sweep_z(typename Tr<R, C
       P *tile = (P *) (base + q * stage_bytes);
       zsweep_tile<R, CPLX, MOM, MSEG, TWC, STAB>(tile, nrows(t), TR, LS, c, p, tbs, blk, part, part2, wz, wz2, hz3,
                                                 rowsum, rowsum2, (long long) t * TR);
-      if (threadIdx.x < 32) copy_tile(t, q, false);
+      if (threadIdx.x == 0) copy_tile(t, q, false);
    }
-   if (threadIdx.x < 32) bulk_wait_all();
+   if (threadIdx.x == 0) bulk_wait_all();
 }
 
 }  // namespace gpe
