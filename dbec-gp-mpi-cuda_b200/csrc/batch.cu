@@ -57,6 +57,9 @@ struct gpe_batch {
    cudaGraphExec_t exec = nullptr;
    long long kernels_per_step = 0;
    long long launches = 0;
+   // a view over handles owned by someone else (the request server), stepping
+   // on the caller's stream: destroying it leaves the handles and the stream
+   bool view = false;
 };
 
 namespace {
@@ -383,14 +386,57 @@ extern "C" gpe_status gpe_batch_create(const gpe_params *params, const double *g
 
 extern "C" void gpe_batch_destroy(gpe_batch *b) {
    if (!b) return;
-   if (!b->inst.empty()) cudaSetDevice(b->dev);
+   cudaSetDevice(b->dev);
    if (b->master) cudaStreamSynchronize(b->master);
    drop_tables(b);
-   for (gpe_solver *s : b->inst) gpe_destroy(s);
+   if (!b->view)
+      for (gpe_solver *s : b->inst) gpe_destroy(s);
    if (b->fork) cudaEventDestroy(b->fork);
-   if (b->master) cudaStreamDestroy(b->master);
+   if (b->master && !b->view) cudaStreamDestroy(b->master);
    delete b;
 }
+
+// ------------------------------------------------------ views (internal.h)
+namespace gpe {
+
+gpe_status batch_view_create(int dev, cudaStream_t stream, gpe_batch **out) {
+   if (!out) return bfail(GPE_ERR_PARAM, "batch view: null output");
+   gpe_batch *b = new gpe_batch();
+   b->view = true;
+   b->dev = dev;
+   b->master = stream;
+   cudaError_t e = cudaSetDevice(dev);
+   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, dev);
+   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+   if (e != cudaSuccess) {
+      delete b;
+      return bfail(GPE_ERR_CUDA, cudaGetErrorString(e));
+   }
+   *out = b;
+   return GPE_OK;
+}
+
+gpe_status batch_view_set(gpe_batch *b, const std::vector<gpe_solver *> &inst, const std::vector<double> &g,
+                          const std::vector<double> &gd) {
+   if (!b || !b->view) return bfail(GPE_ERR_PARAM, "batch view: not a view");
+   drop_tables(b);
+   b->inst = inst;
+   b->g = g;
+   b->gd = gd;
+   return GPE_OK;
+}
+
+gpe_status batch_view_queue(gpe_batch *b, long nsteps) {
+   if (!b || nsteps < 0) return bfail(GPE_ERR_PARAM, "batch view: null or negative step count");
+   if (b->inst.empty() || nsteps == 0) return GPE_OK;
+   BCK(cudaSetDevice(b->dev));
+   if (!b->exec) BCKS(capture(b));
+   for (long c = 0; c < nsteps; c++) BCK(cudaGraphLaunch(b->exec, b->master));
+   b->launches += b->kernels_per_step * nsteps;
+   return GPE_OK;
+}
+
+}  // namespace gpe
 
 extern "C" gpe_status gpe_batch_solver(gpe_batch *b, int i, gpe_solver **s) {
    if (!b || !s || i < 0 || i >= (int) b->inst.size()) return bfail(GPE_ERR_PARAM, "batch: bad instance index");

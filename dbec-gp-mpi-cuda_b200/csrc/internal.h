@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 #include "gpe.h"
 
@@ -31,6 +32,17 @@ long long kernels_per_step(gpe_solver *s);
 // descriptor with those tiles and couplings g, gd.
 struct BatchDesc;
 struct BatchGeom;
+
+// A batch view over handles owned elsewhere (the request server): its steps
+// are queued on `stream` (every handle of the view must use that stream);
+// destroying it (gpe_batch_destroy) leaves the handles and the stream.
+// batch_view_set replaces the members (the step is captured again at the
+// next batch_view_queue); batch_view_queue queues nsteps batched steps and
+// returns without waiting.
+gpe_status batch_view_create(int dev, cudaStream_t stream, gpe_batch **out);
+gpe_status batch_view_set(gpe_batch *b, const std::vector<gpe_solver *> &inst, const std::vector<double> &g,
+                          const std::vector<double> &gd);
+gpe_status batch_view_queue(gpe_batch *b, long nsteps);
 gpe_status batch_geom(gpe_solver *s, int Ly, int Lx, BatchGeom *geom);
 gpe_status batch_desc(gpe_solver *s, int Ly, int Lx, double g, double gd, BatchDesc *out);
 

@@ -1,26 +1,30 @@
 // server.cpp -- request server with continuous batching (gpe_server_* in
 // include/gpe.h).
 //
-// One worker thread owns the GPU work.  Each turn of its loop it
+// One worker thread owns the GPU work.  Active solves live in lanes: a lane
+// holds the solves of one size class (up to 64^3, 128^3, larger), mode and
+// precision, has its own CUDA stream (smaller classes at higher priority)
+// and steps all its solves together with the batched launches of batch.cu
+// (one launch per pass over the lane's descriptor table, captured as one CUDA
+// graph per step).  Each turn of the loop the worker
 //   1. admits queued requests in arrival order while the summed
 //      gpe_device_bytes of the active solves stays within the HBM budget and
 //      fewer than max_active are running (psi is created on the device and
-//      stays there until the request retires);
-//   2. queues the next chunk of steps (plus, for a ground state, its mu) for
-//      active solves that have none in flight, in order of least remaining
-//      work (grid points x steps left), as long as the grid points of the
-//      chunks in flight stay within kFillPoints (the first always goes), each
-//      solve on its own stream with an event recorded behind it: the solves
-//      run side by side on the GPU, each at its own pace, and short requests
-//      are not held behind long ones;
-//   3. polls the chunks' events; for every finished chunk it checks
-//      convergence (ground state: relative change of mu between checks below
-//      tol; evolution: all steps done) and retires finished solves, freeing
-//      their memory for the next admissions.
-// Requests arriving while others run are admitted on the next turn.
-// A solve's arithmetic does not depend on what else is running: every solve
-// has its own handle, stream and buffers, and its chunk boundaries depend only
-// on its own request.
+//      stays there until the request retires); a lane whose membership
+//      changed is captured again before its next chunk;
+//   2. for every lane with no chunk in flight, queues a chunk of batched
+//      steps that ends at the nearest chunk boundary of its members (a
+//      solve's boundaries: every check_every steps and its last step), then,
+//      for the members at a boundary, the pending renormalisation and (ground
+//      state) mu, and an event behind it;
+//   3. polls the lanes' events; at a finished chunk it checks the members at
+//      a boundary (ground state: relative change of mu since the previous
+//      check below tol; evolution: all steps done), retires finished solves
+//      and frees their memory for the next admissions.
+// Requests arriving while others run join a lane at its next chunk boundary.
+// A solve's arithmetic does not depend on what else is running: a batched
+// step is the solve's own step bit for bit, and its renormalisations and mu
+// checks fall on its own boundaries, exactly as when it runs alone.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -29,10 +33,12 @@
 #include <condition_variable>
 #include <deque>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <set>
 #include <string>
 #include <thread>
+#include <tuple>
 #include <vector>
 
 #include "gpe.h"
@@ -41,6 +47,11 @@
 namespace {
 
 using Clock = std::chrono::steady_clock;
+
+int size_class(const gpe_params &p) {
+   const long long n = (long long) p.nx * p.ny * p.nz;
+   return n <= 64LL * 64 * 64 ? 0 : (n <= 128LL * 128 * 128 ? 1 : 2);
+}
 
 struct Active {
    long long id = 0;
@@ -52,17 +63,19 @@ struct Active {
    double t_submit = 0., t_start = 0.;
    gpe_status st = GPE_OK;
    bool done = false;
-   bool inflight = false;
    bool cancel = false;  // gpe_server_cancel: retire at the next chunk boundary
-   cudaEvent_t ev = nullptr;
-   cudaStream_t stream = nullptr;  // created by the server with a priority
+   bool due = false;     // the chunk in flight ends at one of its boundaries
 };
 
-// Grid points of the chunks kept in flight at once: about two 256^3 solves,
-// more than enough to fill the GPU, so admitting more only shares it.
-constexpr long long kFillPoints = 2LL * 256 * 256 * 256;
-
-long long npts_of(const gpe_request &rq) { return (long long) rq.p.nx * rq.p.ny * rq.p.nz; }
+// Solves of one (size class, mode, precision), stepped together.
+struct Lane {
+   cudaStream_t stream = nullptr;
+   gpe_batch *view = nullptr;
+   std::vector<std::unique_ptr<Active>> members;
+   bool dirty = true;  // membership changed since the batch view was set
+   bool inflight = false;
+   cudaEvent_t ev = nullptr;
+};
 
 struct Pending {
    long long id;
@@ -91,9 +104,22 @@ struct gpe_server {
    bool stopping = false;
    double stats[4] = {0, 0, 0, 0};
    std::thread worker;
+   std::map<std::tuple<int, int, int>, Lane> lanes;
+   int nactive = 0;
+   long long used = 0;
 
    double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
 
+   void post(const gpe_result &r) {
+      std::lock_guard<std::mutex> lk(mu);
+      results[r.id] = r;
+      cancel_req.erase(r.id);
+      stats[0] += 1;
+      cv_done.notify_all();
+   }
+
+   // Retires a solve of a lane with no chunk in flight: observables (unless
+   // failed or cancelled), then its memory.
    void finish(Active &a) {
       gpe_result r{};
       r.id = a.id;
@@ -104,6 +130,7 @@ struct gpe_server {
       r.mu = r.en = r.norm = NAN;
       if (a.cancel && a.st == GPE_OK) r.status = GPE_ERR_CANCELLED;
       if (a.st == GPE_OK && !a.cancel) {
+         // the solve ended at a boundary, where its renormalisation was applied
          gpe_status st = gpe::queue_muen(a.s, a.rq.g, a.rq.gd);
          if (st == GPE_OK) st = gpe::read_muen(a.s, &r.mu, &r.en);
          if (st == GPE_OK) st = gpe_calcnorm(a.s, 0, &r.norm);
@@ -112,186 +139,214 @@ struct gpe_server {
       }
       gpe_destroy(a.s);
       a.s = nullptr;
-      if (a.ev) cudaEventDestroy(a.ev);
-      a.ev = nullptr;
-      if (a.stream) cudaStreamDestroy(a.stream);
-      a.stream = nullptr;
+      used -= a.bytes;
+      nactive--;
       r.t_done = now();
-      std::lock_guard<std::mutex> lk(mu);
-      results[a.id] = r;
-      cancel_req.erase(a.id);
-      stats[0] += 1;
-      cv_done.notify_all();
+      post(r);
    }
 
-   // chunk of steps for one active solve
-   long chunk(const Active &a) const {
+   // steps from a's current count to its next boundary
+   static long to_boundary(const Active &a) {
       const long left = a.rq.max_steps - a.steps;
-      return std::max(0L, std::min(a.rq.check_every, left));
+      const long k = a.rq.check_every - a.steps % a.rq.check_every;
+      return std::max(0L, std::min(k, left));
    }
 
-   int prio_lo = 0, prio_mid = 0, prio_hi = 0;
+   void admit(const Pending &pd) {
+      auto a = std::make_unique<Active>();
+      a->id = pd.id;
+      a->rq = pd.rq;
+      a->t_submit = pd.t_submit;
+      a->t_start = now();
+      gpe_device_bytes(&a->rq.p, &a->bytes);
+      if (a->bytes > budget) {
+         a->st = sfail(GPE_ERR_BUDGET, "request exceeds the server's HBM budget");
+      } else {
+         const int cls = size_class(a->rq.p);
+         Lane &L = lanes[std::make_tuple(cls, a->rq.p.mode, a->rq.p.precision)];
+         if (!L.stream) {
+            // smaller classes on higher-priority streams: when the GPU is
+            // shared, the CTA scheduler serves them first, so short requests
+            // are not held back by long ones
+            int least = 0, greatest = 0;
+            cudaDeviceGetStreamPriorityRange(&least, &greatest);
+            const int pr = cls == 0 ? greatest : (cls == 1 ? (least + greatest) / 2 : least);
+            if (cudaStreamCreateWithPriority(&L.stream, cudaStreamNonBlocking, pr) != cudaSuccess ||
+                cudaEventCreateWithFlags(&L.ev, cudaEventDisableTiming) != cudaSuccess)
+               a->st = sfail(GPE_ERR_CUDA, "server: stream creation failed");
+            else
+               a->st = gpe::batch_view_create(device, L.stream, &L.view);
+         }
+         if (a->st == GPE_OK) a->st = gpe_create(&a->rq.p, L.stream, &a->s);
+         if (a->st == GPE_OK) a->st = gpe_init_gaussian(a->s);
+         if (a->st == GPE_OK && a->rq.kind == GPE_REQ_GROUND) {
+            double nrm;
+            a->st = gpe_calcnorm(a->s, 1, &nrm);
+         }
+         if (a->st == GPE_OK) {
+            used += a->bytes;
+            nactive++;
+            L.members.push_back(std::move(a));
+            L.dirty = true;
+            return;
+         }
+      }
+      if (a->s) gpe_destroy(a->s);
+      gpe_result r{};
+      r.id = a->id;
+      r.status = a->st;
+      r.mu = r.en = r.norm = NAN;
+      r.t_submit = a->t_submit;
+      r.t_start = a->t_start;
+      r.t_done = now();
+      post(r);
+   }
+
+   // Queues the next chunk of lane L (no chunk in flight).
+   void launch_chunk(Lane &L) {
+      if (L.members.empty()) return;
+      if (L.dirty) {
+         std::vector<gpe_solver *> inst;
+         std::vector<double> g, gd;
+         for (auto &a : L.members) {
+            inst.push_back(a->s);
+            g.push_back(a->rq.g);
+            gd.push_back(a->rq.gd);
+         }
+         gpe_status st = gpe::batch_view_set(L.view, inst, g, gd);
+         if (st != GPE_OK) {
+            for (auto &a : L.members) {
+               a->st = st;
+               a->done = true;
+            }
+            return;
+         }
+         L.dirty = false;
+      }
+      long n = 1L << 62;
+      for (auto &a : L.members) n = std::min(n, to_boundary(*a));
+      gpe_status st = n > 0 ? gpe::batch_view_queue(L.view, n) : GPE_OK;
+      for (auto &a : L.members) {
+         a->steps += n;
+         a->due = st == GPE_OK && (a->steps % a->rq.check_every == 0 || a->steps >= a->rq.max_steps);
+         if (st != GPE_OK) {
+            a->st = st;
+            a->done = true;
+         } else if (a->due) {
+            a->st = gpe::queue_finish(a->s);
+            if (a->st == GPE_OK && a->rq.kind == GPE_REQ_GROUND) a->st = gpe::queue_muen(a->s, a->rq.g, a->rq.gd);
+            if (a->st != GPE_OK) a->done = true;
+         }
+      }
+      if (cudaEventRecord(L.ev, L.stream) != cudaSuccess) {
+         for (auto &a : L.members) {
+            a->st = sfail(GPE_ERR_CUDA, "server: event record failed");
+            a->done = true;
+         }
+         return;
+      }
+      L.inflight = true;
+      std::lock_guard<std::mutex> lk(mu);
+      stats[3] += 1;
+   }
+
+   // A finished chunk of lane L: checks at the members' boundaries.
+   void chunk_done(Lane &L, cudaError_t q) {
+      L.inflight = false;
+      for (auto &a : L.members) {
+         if (a->done) continue;
+         if (q != cudaSuccess) {
+            a->st = sfail(GPE_ERR_CUDA, cudaGetErrorString(q));
+            a->done = true;
+            continue;
+         }
+         if (!a->due) continue;
+         if (a->rq.kind == GPE_REQ_GROUND) {
+            double m = NAN, e = NAN;
+            a->st = gpe::read_muen(a->s, &m, &e);
+            if (a->st == GPE_OK && std::isfinite(a->mu_prev) && std::fabs(m - a->mu_prev) < a->rq.tol * std::fabs(m))
+               a->done = true;
+            a->mu_prev = m;
+         } else {
+            a->st = gpe_synchronize(a->s);
+         }
+         if (a->steps >= a->rq.max_steps || a->st != GPE_OK) a->done = true;
+      }
+   }
+
+   // Retires the finished and cancelled members of lane L (no chunk in flight).
+   void retire(Lane &L) {
+      {
+         std::lock_guard<std::mutex> lk(mu);
+         for (auto &a : L.members)
+            if (cancel_req.count(a->id)) a->cancel = true;
+      }
+      bool changed = false;
+      for (auto &a : L.members)
+         if (a->done || a->cancel) {
+            finish(*a);
+            changed = true;
+         }
+      if (!changed) return;
+      L.members.erase(std::remove_if(L.members.begin(), L.members.end(),
+                                     [](const std::unique_ptr<Active> &a) { return a->s == nullptr; }),
+                      L.members.end());
+      L.dirty = true;
+   }
 
    void run() {
       cudaSetDevice(device);
-      int least = 0, greatest = 0;
-      if (cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess) {
-         prio_lo = least;
-         prio_hi = greatest;
-         prio_mid = (least + greatest) / 2;
-      }
-      std::vector<Active> active;
-      long long used = 0;
       for (;;) {
          // 1. admission (arrival order, stop at the first that does not fit)
-         std::vector<Pending> admit;
+         std::vector<Pending> admit_now;
          {
             std::unique_lock<std::mutex> lk(mu);
-            if (active.empty() && queue.empty()) {
+            if (nactive == 0 && queue.empty()) {
                if (stopping) break;
                cv_work.wait_for(lk, std::chrono::milliseconds(2));
                continue;
             }
             long long plan = used;
-            while (!queue.empty() && (int) (active.size() + admit.size()) < max_active) {
+            int act = nactive;
+            while (!queue.empty() && act < max_active) {
                long long bytes = 0;
                if (gpe_device_bytes(&queue.front().rq.p, &bytes) != GPE_OK) bytes = 0;
-               if (plan + bytes > budget && !(active.empty() && admit.empty())) break;
+               if (plan + bytes > budget && act > 0) break;
                plan += bytes;
-               admit.push_back(queue.front());
+               act++;
+               admit_now.push_back(queue.front());
                queue.pop_front();
             }
          }
-         for (const Pending &pd : admit) {
-            Active a;
-            a.id = pd.id;
-            a.rq = pd.rq;
-            a.t_submit = pd.t_submit;
-            a.t_start = now();
-            gpe_device_bytes(&a.rq.p, &a.bytes);
-            if (a.bytes > budget) {
-               a.st = sfail(GPE_ERR_BUDGET, "request exceeds the server's HBM budget");
-            } else {
-               // smaller solves on higher-priority streams: when the GPU is
-               // shared, the CTA scheduler serves them first, so short requests
-               // are not held back by long ones (shortest work first)
-               const long long npts = a.rq.p.nx * a.rq.p.ny * a.rq.p.nz;
-               const int pr = npts <= 64 * 64 * 64 ? prio_hi : (npts <= 128 * 128 * 128 ? prio_mid : prio_lo);
-               if (cudaStreamCreateWithPriority(&a.stream, cudaStreamNonBlocking, pr) != cudaSuccess)
-                  a.st = sfail(GPE_ERR_CUDA, "server: stream creation failed");
-               else
-                  a.st = gpe_create(&a.rq.p, a.stream, &a.s);
-               if (a.st == GPE_OK) a.st = gpe_init_gaussian(a.s);
-               if (a.st == GPE_OK && a.rq.kind == GPE_REQ_GROUND) {
-                  double nrm;
-                  a.st = gpe_calcnorm(a.s, 1, &nrm);
-               }
-            }
-            if (a.st != GPE_OK) {
-               if (a.s) {
-                  gpe_destroy(a.s);
-                  a.s = nullptr;
-               }
-               if (a.stream) cudaStreamDestroy(a.stream);
-               gpe_result r{};
-               r.id = a.id;
-               r.status = a.st;
-               r.t_submit = a.t_submit;
-               r.t_start = a.t_start;
-               r.t_done = now();
-               std::lock_guard<std::mutex> lk(mu);
-               results[a.id] = r;
-               cancel_req.erase(a.id);
-               stats[0] += 1;
-               cv_done.notify_all();
-               continue;
-            }
-            used += a.bytes;
-            active.push_back(a);
-         }
+         for (const Pending &pd : admit_now) admit(pd);
          {
             std::lock_guard<std::mutex> lk(mu);
-            stats[1] = std::max(stats[1], (double) active.size());
+            stats[1] = std::max(stats[1], (double) nactive);
             stats[2] = std::max(stats[2], (double) used);
          }
-         if (active.empty()) continue;
-         // cancellations: a solve stops at its next chunk boundary (never with
-         // a chunk of its kernels in flight)
-         {
-            std::lock_guard<std::mutex> lk(mu);
-            for (Active &a : active)
-               if (cancel_req.count(a.id)) a.cancel = true;
-         }
-         for (Active &a : active)
-            if (a.cancel && !a.inflight) a.done = true;
-         // 2. next chunks, least remaining work first, within the fill budget
-         long long fill = 0;
-         for (const Active &a : active)
-            if (a.inflight) fill += npts_of(a.rq);
-         std::vector<Active *> order;
-         for (Active &a : active)
-            if (!a.inflight && !a.done) order.push_back(&a);
-         std::sort(order.begin(), order.end(), [](const Active *x, const Active *y) {
-            return npts_of(x->rq) * (x->rq.max_steps - x->steps) < npts_of(y->rq) * (y->rq.max_steps - y->steps);
-         });
-         for (Active *ap : order) {
-            Active &a = *ap;
-            if (fill > 0 && fill + npts_of(a.rq) > kFillPoints) continue;
-            fill += npts_of(a.rq);
-            if (!a.ev && cudaEventCreateWithFlags(&a.ev, cudaEventDisableTiming) != cudaSuccess) {
-               a.st = sfail(GPE_ERR_CUDA, "server: event creation failed");
-               a.done = true;
-               continue;
-            }
-            const long n = chunk(a);
-            a.st = gpe::queue_steps(a.s, n, a.rq.g, a.rq.gd);
-            if (a.st == GPE_OK) a.st = gpe::queue_finish(a.s);
-            if (a.st == GPE_OK && a.rq.kind == GPE_REQ_GROUND) a.st = gpe::queue_muen(a.s, a.rq.g, a.rq.gd);
-            if (a.st == GPE_OK && cudaEventRecord(a.ev, gpe::stream_of(a.s)) != cudaSuccess)
-               a.st = sfail(GPE_ERR_CUDA, "server: event record failed");
-            a.steps += n;
-            if (a.st != GPE_OK) {
-               a.done = true;
-               continue;
-            }
-            a.inflight = true;
-            std::lock_guard<std::mutex> lk(mu);
-            stats[3] += 1;
-         }
-         // 3. finished chunks: check, retire
+         // 2./3. per lane: a finished chunk is checked, finished solves
+         // retire, the next chunk goes out
          bool progressed = false;
-         for (Active &a : active) {
-            if (!a.inflight) continue;
-            const cudaError_t q = cudaEventQuery(a.ev);
-            if (q == cudaErrorNotReady) continue;
-            a.inflight = false;
-            progressed = true;
-            if (q != cudaSuccess) {
-               a.st = sfail(GPE_ERR_CUDA, cudaGetErrorString(q));
-               a.done = true;
-               continue;
+         for (auto &kv : lanes) {
+            Lane &L = kv.second;
+            if (L.inflight) {
+               const cudaError_t q = cudaEventQuery(L.ev);
+               if (q == cudaErrorNotReady) continue;
+               chunk_done(L, q);
+               progressed = true;
             }
-            if (a.rq.kind == GPE_REQ_GROUND) {
-               double m = NAN, e = NAN;
-               a.st = gpe::read_muen(a.s, &m, &e);
-               if (a.st == GPE_OK && std::isfinite(a.mu_prev) && std::fabs(m - a.mu_prev) < a.rq.tol * std::fabs(m))
-                  a.done = true;
-               a.mu_prev = m;
-            } else {
-               a.st = gpe_synchronize(a.s);
-            }
-            if (a.steps >= a.rq.max_steps || a.st != GPE_OK || a.cancel) a.done = true;
+            retire(L);
+            launch_chunk(L);
          }
-         for (Active &a : active)
-            if (a.done && !a.inflight) {
-               used -= a.bytes;
-               finish(a);
-            }
-         active.erase(std::remove_if(active.begin(), active.end(),
-                                     [](const Active &a) { return a.done && !a.inflight && !a.s; }),
-                      active.end());
          if (!progressed) std::this_thread::sleep_for(std::chrono::microseconds(50));
       }
+      for (auto &kv : lanes) {
+         Lane &L = kv.second;
+         if (L.view) gpe_batch_destroy(L.view);
+         if (L.ev) cudaEventDestroy(L.ev);
+         if (L.stream) cudaStreamDestroy(L.stream);
+      }
+      lanes.clear();
    }
 };
 
@@ -375,7 +430,7 @@ extern "C" gpe_status gpe_server_cancel(gpe_server *sv, long long id) {
          sv->cv_done.notify_all();
          return GPE_OK;
       }
-   sv->cancel_req.insert(id);  // admitted: the worker retires it at the next chunk boundary
+   sv->cancel_req.insert(id);  // admitted: retired at its lane's next chunk boundary
    return GPE_OK;
 }
 
