@@ -10,13 +10,15 @@
 //   1. admits queued requests in arrival order while the summed
 //      gpe_device_bytes of the active solves stays within the HBM budget and
 //      fewer than max_active are running (psi is created on the device and
-//      stays there until the request retires); a lane whose membership
+//      stays there until the request retires); a lane whose stepping set
 //      changed is captured again before its next chunk;
 //   2. for every lane with no chunk in flight, queues a chunk of batched
-//      steps that ends at the nearest chunk boundary of its members (a
-//      solve's boundaries: every check_every steps and its last step), then,
-//      for the members at a boundary, the pending renormalisation and (ground
-//      state) mu, and an event behind it;
+//      steps for the members with the least remaining work whose grid points
+//      fit the lane's budget (shortest first; the others wait, resident),
+//      ending at the nearest chunk boundary of those members (a solve's
+//      boundaries: every check_every steps and its last step), then, for the
+//      members at a boundary, the pending renormalisation and (ground state)
+//      mu, and an event behind it;
 //   3. polls the lanes' events; at a finished chunk it checks the members at
 //      a boundary (ground state: relative change of mu since the previous
 //      check below tol; evolution: all steps done), retires finished solves
@@ -65,14 +67,23 @@ struct Active {
    bool done = false;
    bool cancel = false;  // gpe_server_cancel: retire at the next chunk boundary
    bool due = false;     // the chunk in flight ends at one of its boundaries
+   bool on = false;      // stepping in the current chunk
 };
+
+// Grid points a lane steps at once: about two 256^3 solves, enough to fill
+// the GPU; beyond that, stepping more solves together only shares it, so the
+// lane steps the solves with the least remaining work (shortest first) and
+// the others wait, resident, for their turn.
+constexpr long long kLanePoints = 2LL * 256 * 256 * 256;
+
+long long npts_of(const gpe_request &rq) { return (long long) rq.p.nx * rq.p.ny * rq.p.nz; }
 
 // Solves of one (size class, mode, precision), stepped together.
 struct Lane {
    cudaStream_t stream = nullptr;
    gpe_batch *view = nullptr;
    std::vector<std::unique_ptr<Active>> members;
-   bool dirty = true;  // membership changed since the batch view was set
+   std::vector<Active *> stepping;  // the members of the batch view
    bool inflight = false;
    cudaEvent_t ev = nullptr;
 };
@@ -187,7 +198,6 @@ struct gpe_server {
             used += a->bytes;
             nactive++;
             L.members.push_back(std::move(a));
-            L.dirty = true;
             return;
          }
       }
@@ -202,13 +212,28 @@ struct gpe_server {
       post(r);
    }
 
-   // Queues the next chunk of lane L (no chunk in flight).
+   // Queues the next chunk of lane L (no chunk in flight): the members with
+   // the least remaining work (grid points x steps left) while their points
+   // fit kLanePoints (the first always) step to the nearest of their
+   // boundaries.
    void launch_chunk(Lane &L) {
       if (L.members.empty()) return;
-      if (L.dirty) {
+      std::vector<Active *> order;
+      for (auto &a : L.members) order.push_back(a.get());
+      std::stable_sort(order.begin(), order.end(), [](const Active *x, const Active *y) {
+         return npts_of(x->rq) * (x->rq.max_steps - x->steps) < npts_of(y->rq) * (y->rq.max_steps - y->steps);
+      });
+      std::vector<Active *> sel;
+      long long pts = 0;
+      for (Active *a : order) {
+         if (!sel.empty() && pts + npts_of(a->rq) > kLanePoints) continue;
+         sel.push_back(a);
+         pts += npts_of(a->rq);
+      }
+      if (sel != L.stepping) {
          std::vector<gpe_solver *> inst;
          std::vector<double> g, gd;
-         for (auto &a : L.members) {
+         for (Active *a : sel) {
             inst.push_back(a->s);
             g.push_back(a->rq.g);
             gd.push_back(a->rq.gd);
@@ -219,14 +244,17 @@ struct gpe_server {
                a->st = st;
                a->done = true;
             }
+            L.stepping.clear();
             return;
          }
-         L.dirty = false;
+         L.stepping = sel;
       }
+      for (auto &a : L.members) a->on = a->due = false;
       long n = 1L << 62;
-      for (auto &a : L.members) n = std::min(n, to_boundary(*a));
+      for (Active *a : sel) n = std::min(n, to_boundary(*a));
       gpe_status st = n > 0 ? gpe::batch_view_queue(L.view, n) : GPE_OK;
-      for (auto &a : L.members) {
+      for (Active *a : sel) {
+         a->on = true;
          a->steps += n;
          a->due = st == GPE_OK && (a->steps % a->rq.check_every == 0 || a->steps >= a->rq.max_steps);
          if (st != GPE_OK) {
@@ -254,13 +282,13 @@ struct gpe_server {
    void chunk_done(Lane &L, cudaError_t q) {
       L.inflight = false;
       for (auto &a : L.members) {
-         if (a->done) continue;
+         if (a->done || !a->on) continue;
          if (q != cudaSuccess) {
             a->st = sfail(GPE_ERR_CUDA, cudaGetErrorString(q));
             a->done = true;
             continue;
          }
-         if (!a->due) continue;
+         if (!a->on || !a->due) continue;
          if (a->rq.kind == GPE_REQ_GROUND) {
             double m = NAN, e = NAN;
             a->st = gpe::read_muen(a->s, &m, &e);
@@ -291,7 +319,7 @@ struct gpe_server {
       L.members.erase(std::remove_if(L.members.begin(), L.members.end(),
                                      [](const std::unique_ptr<Active> &a) { return a->s == nullptr; }),
                       L.members.end());
-      L.dirty = true;
+      L.stepping.clear();  // the view is set again before the next chunk
    }
 
    void run() {
