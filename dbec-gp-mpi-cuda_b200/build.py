@@ -56,7 +56,8 @@ def _run(cmd):
 
 def build_lib(force=False, verbose_ptxas=False):
     """Compiles the library's translation units in parallel (each depends on
-    every header, so a header change rebuilds them all), then links."""
+    its source and every header, so a header change rebuilds them all), then
+    links."""
     from concurrent.futures import ThreadPoolExecutor
     os.makedirs(LIB_DIR, exist_ok=True)
     os.makedirs(OBJ_DIR, exist_ok=True)
@@ -65,8 +66,9 @@ def build_lib(force=False, verbose_ptxas=False):
         return LIB
     extra = ["-Xptxas", "-v"] if verbose_ptxas else []
     objs = [os.path.join(OBJ_DIR, f + ".o") for f in LIB_SOURCES]
+    headers = [d for d in deps if not d.endswith((".cu", ".cpp"))]
     jobs = [[NVCC] + NVFLAGS + extra + ["-c", "-o", o, os.path.join(CSRC, f)]
-            for f, o in zip(LIB_SOURCES, objs) if force or _stale(o, deps)]
+            for f, o in zip(LIB_SOURCES, objs) if force or _stale(o, headers + [os.path.join(CSRC, f)])]
     with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
         list(ex.map(_run, jobs))
     _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lpthread"])

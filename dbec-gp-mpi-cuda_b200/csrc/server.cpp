@@ -12,9 +12,10 @@
 //      fewer than max_active are running (psi is created on the device and
 //      stays there until the request retires); a lane whose stepping set
 //      changed is captured again before its next chunk;
-//   2. for every lane with no chunk in flight, queues a chunk of batched
-//      steps for the members with the least remaining work whose grid points
-//      fit the lane's budget (shortest first; the others wait, resident),
+//   2. for every lane with no chunk in flight (smallest size class first),
+//      queues a chunk of batched steps for the members with the least
+//      remaining work while the grid points in flight over all lanes stay
+//      within a budget of about two 256^3 solves (the others wait, resident),
 //      ending at the nearest chunk boundary of those members (a solve's
 //      boundaries: every check_every steps and its last step), then, for the
 //      members at a boundary, the pending renormalisation and (ground state)
@@ -70,11 +71,11 @@ struct Active {
    bool on = false;      // stepping in the current chunk
 };
 
-// Grid points a lane steps at once: about two 256^3 solves, enough to fill
-// the GPU; beyond that, stepping more solves together only shares it, so the
-// lane steps the solves with the least remaining work (shortest first) and
-// the others wait, resident, for their turn.
-constexpr long long kLanePoints = 2LL * 256 * 256 * 256;
+// Grid points stepping at once over all lanes: about two 256^3 solves,
+// enough to fill the GPU; beyond that, stepping more solves together only
+// shares it, so the solves with the least remaining work step first and the
+// others wait, resident, for their turn.
+constexpr long long kFillPoints = 2LL * 256 * 256 * 256;
 
 long long npts_of(const gpe_request &rq) { return (long long) rq.p.nx * rq.p.ny * rq.p.nz; }
 
@@ -84,6 +85,7 @@ struct Lane {
    gpe_batch *view = nullptr;
    std::vector<std::unique_ptr<Active>> members;
    std::vector<Active *> stepping;  // the members of the batch view
+   long long pts = 0;               // grid points of the chunk in flight
    bool inflight = false;
    cudaEvent_t ev = nullptr;
 };
@@ -214,9 +216,10 @@ struct gpe_server {
 
    // Queues the next chunk of lane L (no chunk in flight): the members with
    // the least remaining work (grid points x steps left) while their points
-   // fit kLanePoints (the first always) step to the nearest of their
-   // boundaries.
-   void launch_chunk(Lane &L) {
+   // fit `avail` (the first also when nothing else is in flight) step to the
+   // nearest of their boundaries.
+   void launch_chunk(Lane &L, long long avail, bool first_always) {
+      L.pts = 0;
       if (L.members.empty()) return;
       std::vector<Active *> order;
       for (auto &a : L.members) order.push_back(a.get());
@@ -226,10 +229,11 @@ struct gpe_server {
       std::vector<Active *> sel;
       long long pts = 0;
       for (Active *a : order) {
-         if (!sel.empty() && pts + npts_of(a->rq) > kLanePoints) continue;
+         if (pts + npts_of(a->rq) > avail && !(sel.empty() && first_always)) continue;
          sel.push_back(a);
          pts += npts_of(a->rq);
       }
+      if (sel.empty()) return;  // waits for budget
       if (sel != L.stepping) {
          std::vector<gpe_solver *> inst;
          std::vector<double> g, gd;
@@ -274,6 +278,7 @@ struct gpe_server {
          return;
       }
       L.inflight = true;
+      L.pts = pts;
       std::lock_guard<std::mutex> lk(mu);
       stats[3] += 1;
    }
@@ -357,14 +362,23 @@ struct gpe_server {
          bool progressed = false;
          for (auto &kv : lanes) {
             Lane &L = kv.second;
-            if (L.inflight) {
-               const cudaError_t q = cudaEventQuery(L.ev);
-               if (q == cudaErrorNotReady) continue;
-               chunk_done(L, q);
-               progressed = true;
-            }
+            if (!L.inflight) continue;
+            const cudaError_t q = cudaEventQuery(L.ev);
+            if (q == cudaErrorNotReady) continue;
+            chunk_done(L, q);
+            progressed = true;
+         }
+         // lanes in size-class order (smallest first) share one budget of
+         // grid points in flight
+         long long busy = 0;
+         for (auto &kv : lanes)
+            if (kv.second.inflight) busy += kv.second.pts;
+         for (auto &kv : lanes) {
+            Lane &L = kv.second;
+            if (L.inflight) continue;
             retire(L);
-            launch_chunk(L);
+            launch_chunk(L, kFillPoints - busy, busy == 0);
+            busy += L.pts;
          }
          if (!progressed) std::this_thread::sleep_for(std::chrono::microseconds(50));
       }
