@@ -265,8 +265,8 @@ __global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) kb_sweep_xy(const
          copy_view(sv, D.sv[AXIS]);
          if constexpr (NU && AXIS == 0 && std::is_same<R, double>::value) {
             const SweepView &v = D.sv[AXIS];
-            const double *src = !CPLX ? (const double *) v.lin.ex : v.trap.x2;
-            for (int e = threadIdx.x; e < v.tb.n; e += blockDim.x) xtab[e] = src[e];
+            const double *src = (const double *) v.lin.ex;
+            for (int e = threadIdx.x; e < (CPLX ? 2 : 1) * v.tb.n; e += blockDim.x) xtab[e] = src[e];
          }
          cur = i;
       }

@@ -407,7 +407,7 @@ static gpe_status plan_tiles(gpe_solver *s) {
             const long rows = (long) std::min<long>(nn[ax], 256) * ((nn[ax] + 255) / 256);
             stage = (rows * TW * esz + (ax == 0 ? rows * TW * rsz : 0) + 127) & ~(size_t) 127;
             // FP64 x sweep: calcnu's per-x table staged in shared memory
-            fixed = 128 + blk + (ax == 0 && !s->fp32 ? (size_t) nn[0] * sizeof(double) : 0);
+            fixed = 128 + blk + (ax == 0 && !s->fp32 ? (size_t) nn[0] * (s->cplx ? 16 : 8) : 0);
          } else {
             stage = ((size_t) TW * (d.nz + 16 / esz) * esz + 127) & ~(size_t) 127;
             // FP64: the four coefficient tables staged in shared memory
@@ -656,7 +656,24 @@ static gpe_status create_impl(const gpe_params *p, void *stream, gpe_solver *s) 
          *dst[a] = (float *) t;
       }
    }
-   // trap factors per axis for calcnu in imaginary time: exp(-dt 0.5 par c x^2)
+   // trap factors per axis for calcnu: exp(-dt 0.5 par c x^2) in imaginary
+   // time; in real time (FP64) the phases exp(-i dt 0.5 par c x^2), stored as
+   // (cos, sin) pairs
+   if (s->cplx && !s->fp32) {
+      const long double hp = 0.5L * (long double) s->par, dt = (long double) p->dt;
+      const long double cf[3] = {(long double) p->gamma * p->gamma, (long double) p->nu * p->nu,
+                                 (long double) p->lambda * p->lambda};
+      const std::vector<double> *sq[3] = {&s->hx2, &s->hy2, &s->hz2};
+      for (int a = 0; a < 3; a++) {
+         const size_t n = sq[a]->size();
+         std::vector<double2> tab(n);
+         for (size_t i = 0; i < n; i++) {
+            const long double th = -dt * hp * cf[a] * (long double) (*sq[a])[i];
+            tab[i] = make_double2((double) cosl(th), (double) sinl(th));
+         }
+         CKS(upload(&s->lin[a], tab.data(), tab.size()));
+      }
+   }
    if (!s->cplx) {
       const long double hp = 0.5L * (long double) s->par, dt = (long double) p->dt;
       const long double cf[3] = {(long double) p->gamma * p->gamma, (long double) p->nu * p->nu,
@@ -1113,7 +1130,7 @@ template <class R, bool CPLX> struct Impl {
          g->stage[ax] = (uint32_t) ((stage + 127) & ~(size_t) 127);
          g->blk[ax] = (uint32_t) ((2 * (size_t) ((P + spw - 1) / spw + 1) * TW * esz + 15) & ~(size_t) 15);
          if (!s->fp32) {
-            if (ax == 0) g->extra[ax] = (uint32_t) (d.nx * sizeof(double));
+            if (ax == 0) g->extra[ax] = (uint32_t) (d.nx * (s->cplx ? 16 : 8));
             if (ax == 2) g->extra[ax] = (uint32_t) (4 * (size_t) d.nz * (s->cplx ? 16 : 8));
          }
          if (ax == 2) g->part = (uint32_t) (((size_t) P * TW * sizeof(double) + 15) & ~(size_t) 15);

@@ -255,13 +255,42 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
    if (simp2) *simp2 = acc2;
 }
 
+// exp(-i t) = (cos t, -sin t) for the nonlinear part of the real-time phase,
+// which is small in practice: Maclaurin series on |t| <= 0.25 (through t^11
+// for sin and t^12 for cos; the first omitted terms are below 3e-18), the
+// library sincos beyond.
+__device__ __forceinline__ double2 expi_small(double t) {
+   if (fabs(t) > 0.25) {
+      double sn, cs;
+      sincos(-t, &sn, &cs);
+      return make_double2(cs, sn);
+   }
+   constexpr double s3 = 1. / 6, s5 = s3 / 20, s7 = s5 / 42, s9 = s7 / 72, s11 = s9 / 110;
+   constexpr double c2 = 1. / 2, c4 = c2 / 12, c6 = c4 / 30, c8 = c6 / 56, c10 = c8 / 90, c12 = c10 / 132;
+   const double t2 = t * t;
+   double sp = fma(-s11, t2, s9);
+   sp = fma(sp, t2, -s7);
+   sp = fma(sp, t2, s5);
+   sp = fma(sp, t2, -s3);
+   const double sn = fma(sp * t2, t, t);
+   double cp = fma(c12, t2, -c10);
+   cp = fma(cp, t2, c8);
+   cp = fma(cp, t2, -c6);
+   cp = fma(cp, t2, c4);
+   cp = fma(cp, t2, -c2);
+   const double cs = fma(cp, t2, 1.);
+   return make_double2(cs, -sn);
+}
+
 // FP64 calcnu over a staged tile before its sweep (the x sweep's fused
 // calcnu_kernel, imag3d-mpicuda.cu:1759, real3d-mpicuda.cu:1856), one z
 // column per thread, with the pending 1/norm applied first.  Tile t of the
 // sweep covers z columns [z0, z0 + TW) of plane `other` (y for the x sweep,
 // x for the y sweep); xtab is calcnu's per-x table staged in shared memory
-// (imaginary time: exp(-dt V_x); real time: x^2).  The caller synchronises
-// the CTA afterwards.
+// (imaginary time: exp(-dt V_x); real time: the phase exp(-i dt V_x)).  The
+// trap part of the exponent is a product of per-axis factors (V is a sum
+// over the axes), so only the nonlinear part is evaluated per point, by a
+// series.  The caller synchronises the CTA afterwards.
 template <class R, bool CPLX, int AXIS>
 __device__ __forceinline__ void nu_pass_fp64(typename Tr<R, CPLX>::P *tile, const R *ptile, int n, int lg, int c,
                                              int other, int z0, const Dims &d, const Trap &trap, const LinPhase &lin,
@@ -280,6 +309,17 @@ __device__ __forceinline__ void nu_pass_fp64(typename Tr<R, CPLX>::P *tile, cons
          const int e = (ii << lg) + c;
          const double lx = xtab[ii] * eyz;
          tile[e] = nu_split(scl(tile[e], scale), (double) ptile[e], lx, g, gd, dt, (double) invN);
+      }
+   } else if constexpr (CPLX && AXIS == 0) {
+      // real time: psi exp(-i dt V_x) exp(-i dt (V_y + V_z)) exp(-i dt (g |psi|^2 + gd phi / N))
+      const double2 ey = __ldg((const double2 *) lin.ey + other), ez = __ldg((const double2 *) lin.ez + k);
+      const double2 eyz = cmul(ey, ez);
+      const double2 *ex = (const double2 *) xtab;
+      for (int ii = threadIdx.x >> lg; ii < n; ii += step) {
+         const int e = (ii << lg) + c;
+         const double2 p = scl(tile[e], scale);
+         const double thn = dt * fma(fma(p.x, p.x, p.y * p.y), g, ((double) ptile[e] * invN) * gd);
+         tile[e] = cmul(p, cmul(cmul(ex[ii], eyz), expi_small(thn)));
       }
    } else {
       // Trap::v with the terms of the two fixed coordinates hoisted
@@ -423,14 +463,16 @@ __global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) k_sweep_xy(const 
       }
       if (!load) bulk_commit();
    };
-   // FP64: calcnu's per-x factor (trap x^2, or exp(-dt V_x) in imaginary
-   // time) staged once per CTA after the block maps, the shared tiles leaving
-   // little L1 for the tables (real-time x sweep 223 -> 219 us at 256^3; the
-   // FP32 sweep measured no faster with it and reads the table from global)
+   // FP64: calcnu's per-x factor (the phase exp(-i dt V_x) in real time,
+   // exp(-dt V_x) in imaginary time) staged once per CTA after the block
+   // maps, the shared tiles leaving little L1 for the tables (real-time x
+   // sweep 223 -> 219 us at 256^3 when it held x^2; the FP32 sweep reads its
+   // tables from global)
    double *xtab = (double *) (blk + 2 * (((tb.P + 32 / TW - 1) / (32 / TW)) + 1) * TW);
    if constexpr (NU && AXIS == 0 && std::is_same<R, double>::value) {
-      const double *src = !CPLX ? (const double *) lin.ex : trap.x2;
-      for (int e = threadIdx.x; e < n; e += blockDim.x) xtab[e] = src[e];
+      // imaginary time: exp(-dt V_x); real time: (cos, sin) of -dt V_x
+      const double *src = (const double *) lin.ex;
+      for (int e = threadIdx.x; e < (CPLX ? 2 : 1) * n; e += blockDim.x) xtab[e] = src[e];
    }
    if (threadIdx.x == 0) {
       for (int q = 0; q < S; q++) mbar_init(&full[q], 1);
