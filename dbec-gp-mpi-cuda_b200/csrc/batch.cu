@@ -167,7 +167,7 @@ gpe_status build_tables(gpe_batch *b) {
          size_t sm = 128 + 2 * (size_t) A.stage[a] + A.blk[a] + A.extra[a];
          if (a == 2) sm += 2 * (size_t) A.part;
          if (sm > kSmemCap) return bfail(GPE_ERR_PARAM, "batch: sweep tiles exceed shared memory");
-         const int cap = G.fp32 ? sweep_ctas<float>(a == 0) : sweep_ctas<double>(a == 0);
+         const int cap = a == 0 ? kSweepCtas[1] : kSweepCtas[0];
          const int ctas = std::max(1, std::min(cap, (int) (kSmemCap / sm)));
          G.sweep_smem[a] = sm;
          G.sweep_grid[a] = (int) std::min<long long>(A.tiles[kPXsweep + a], (long long) ctas * b->nsm);
@@ -218,6 +218,8 @@ template <class R, bool CPLX> struct BatchStep {
       return f(std::integral_constant<int, 2>());
    }
    template <class F> static gpe_status with_mseg(int m, F f) {
+      if constexpr (std::is_same<R, float>::value && !CPLX)
+         if (m > 16) return f(std::integral_constant<int, 32>());
       if (m > 8) return f(std::integral_constant<int, 16>());
       return f(std::integral_constant<int, 8>());
    }

@@ -192,7 +192,7 @@ __device__ __forceinline__ void copy_view(SweepView &dst, const SweepView &src) 
 }
 
 template <class R, bool CPLX, int AXIS, bool NU, int MSEG, int S>
-__global__ void __launch_bounds__(256, sweep_ctas<R>(NU)) kb_sweep_xy(const BatchDesc *__restrict__ tab,
+__global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) kb_sweep_xy(const BatchDesc *__restrict__ tab,
                                                                            const unsigned *__restrict__ work,
                                                                            int ntiles, uint32_t stage_bytes,
                                                                            uint32_t blk_bytes) {
@@ -277,19 +277,12 @@ __global__ void __launch_bounds__(256, sweep_ctas<R>(NU)) kb_sweep_xy(const Batc
       const int other = r.local / nzb, z0 = (r.local - other * nzb) * TW;
       P *tile = (P *) (base + q * stage_bytes);
       const double scale = NU ? sv.st->scale : 1.;
-      if constexpr (NU && std::is_same<R, double>::value && !CPLX) {
+      if constexpr (NU && std::is_same<R, double>::value) {
          nu_pass_fp64<R, CPLX, AXIS>(tile, (const R *) (tile + rows * TW), sv.tb.n, lg, c, other, z0, sv.d, sv.trap,
                                      sv.lin, xtab, sv.g, sv.gd, sv.dt, scale);
          __syncthreads();
       }
-      if constexpr (NU && std::is_same<R, double>::value && CPLX) {
-         static_assert(AXIS == 0, "calcnu is fused into the x sweep only");
-         const int k = min(z0 + c, sv.d.nz - 1);
-         const NuPhase64 xf{(const double *) (tile + rows * TW) + c, TW, (const double2 *) xtab,
-                            cmul(__ldg((const double2 *) sv.lin.ey + other), __ldg((const double2 *) sv.lin.ez + k)),
-                            scale, sv.g, sv.gd, sv.dt, 1.0 / (double) sv.d.npts};
-         seg_sweep<R, CPLX, MSEG, 0>(tile, TW, 1, c, p, TW, sv.tb, blk, nullptr, nullptr, nullptr, nullptr, xf);
-      } else if constexpr (NU && std::is_same<R, float>::value) {
+      if constexpr (NU && std::is_same<R, float>::value) {
          static_assert(AXIS == 0, "calcnu is fused into the x sweep only");
          const NuTrap32<CPLX> xf = nu_reads_fp32<CPLX>((const float *) (tile + rows * TW) + c, TW, other, z0, c, sv.d,
                                                        sv.trap, sv.lin, sv.g, sv.gd, sv.dt, scale);
@@ -305,7 +298,7 @@ __global__ void __launch_bounds__(256, sweep_ctas<R>(NU)) kb_sweep_xy(const Batc
 }
 
 template <class R, bool CPLX, int MOM, int MSEG, int S>
-__global__ void __launch_bounds__(256, sweep_ctas<R>(false)) kb_sweep_z(const BatchDesc *__restrict__ tab,
+__global__ void __launch_bounds__(256, kSweepCtas[0]) kb_sweep_z(const BatchDesc *__restrict__ tab,
                                                                  const unsigned *__restrict__ work, int ntiles,
                                                                  uint32_t stage_bytes, uint32_t blk_bytes,
                                                                  uint32_t part_bytes) {

@@ -366,13 +366,12 @@ static gpe_status make_tmap(CUtensorMap *m, void *base, size_t esz, long w_nz, l
 // Candidate (lines per CTA TW, segment length MSEG, segments P) for a sweep
 // over lines of length n, widest tile first: TW from `tw_base` (a 128-byte
 // row) down to 2, at most 256 threads (TW * P).  Lines of 16-byte elements
-// (FP64 complex) keep 8-point segments (16 would spill the FP64 register
-// budget), and so do FP32 complex lines (the FP32 budget is half the FP64
-// one); FP64 and FP32 real lines may use 16-point segments.
-static int sweep_candidates(int n, int tw_base, int esz, bool fp32, int *TW, int *MSEG, int *P, int cap) {
-   const bool wide = esz == 16 || (fp32 && esz == 8);
-   const int ms[2] = {8, 16};
-   const int nms = wide ? 1 : 2;
+// keep 8-point segments (16 would spill registers); 4-byte elements may use
+// 32-point segments, which keep 64-byte tile rows on 512-point lines.
+static int sweep_candidates(int n, int tw_base, int esz, int *TW, int *MSEG, int *P, int cap) {
+   const bool wide = esz == 16;
+   const int ms[3] = {8, 16, 32};
+   const int nms = wide ? 1 : (esz == 4 ? 3 : 2);
    int k = 0;
    for (int tw = tw_base; tw >= 2 && k < cap; tw /= 2)
       for (int mi = 0; mi < nms && k < cap; mi++) {
@@ -398,9 +397,9 @@ static gpe_status plan_tiles(gpe_solver *s) {
       auto &w = s->sw[ax];
       // the widest tile for which as many CTAs as the kernels are compiled for
       // fit on an SM with a 2-stage pipeline (else the widest tile, fewer CTAs)
-      const int max_ctas = s->fp32 ? sweep_ctas<float>(ax == 0) : sweep_ctas<double>(ax == 0);
+      const int max_ctas = kSweepCtas[ax == 0 ? 1 : 0];
       int cTW[8], cM[8], cP[8];
-      const int nc = sweep_candidates((int) nn[ax], tw_base, (int) esz, s->fp32, cTW, cM, cP, 8);
+      const int nc = sweep_candidates((int) nn[ax], tw_base, (int) esz, cTW, cM, cP, 8);
       auto sizes = [&](int TW, int P, size_t &stage, size_t &fixed) {
          const int spw = 32 / TW;
          const size_t blk = 2 * (size_t) ((P + spw - 1) / spw + 1) * TW * esz;
@@ -930,8 +929,14 @@ template <class R, bool CPLX> struct Impl {
       return sweep_xy_launch_t<AXIS, NU, MSEG, S, 0>(s, g, gd);
    }
 
+   // 32-point segments exist for FP32 real lines only (register budget)
+   static constexpr bool kSeg32 = std::is_same<R, float>::value && !CPLX;
+
    template <int AXIS, bool NU> static gpe_status sweep_xy(gpe_solver *s, double g, double gd) {
       const auto &w = s->sw[AXIS];
+      if constexpr (kSeg32)
+         if (w.MSEG == 32)
+            return w.S == 3 ? sweep_xy_launch<AXIS, NU, 32, 3>(s, g, gd) : sweep_xy_launch<AXIS, NU, 32, 2>(s, g, gd);
       if (w.MSEG == 8) return w.S == 3 ? sweep_xy_launch<AXIS, NU, 8, 3>(s, g, gd) : sweep_xy_launch<AXIS, NU, 8, 2>(s, g, gd);
       return w.S == 3 ? sweep_xy_launch<AXIS, NU, 16, 3>(s, g, gd) : sweep_xy_launch<AXIS, NU, 16, 2>(s, g, gd);
    }
@@ -969,6 +974,8 @@ template <class R, bool CPLX> struct Impl {
 
    template <int MOM> static gpe_status zsweep_m(gpe_solver *s) {
       const auto &w = s->sw[2];
+      if constexpr (kSeg32)
+         if (w.MSEG == 32) return w.S == 3 ? sweep_z_launch<MOM, 32, 3>(s) : sweep_z_launch<MOM, 32, 2>(s);
       if (w.MSEG == 8) return w.S == 3 ? sweep_z_launch<MOM, 8, 3>(s) : sweep_z_launch<MOM, 8, 2>(s);
       return w.S == 3 ? sweep_z_launch<MOM, 16, 3>(s) : sweep_z_launch<MOM, 16, 2>(s);
    }
@@ -1763,7 +1770,7 @@ extern "C" gpe_status gpe_autotune(gpe_solver *s, double g, double gd, int nstep
       const long nn[3] = {s->d.nx, s->d.ny, s->d.nz};
       int cTW[3][8], cM[8], cP[8], nc[3];
       for (int a = 0; a < 3; a++)
-         nc[a] = sweep_candidates((int) nn[a], (int) (128 / s->esz_psi), (int) s->esz_psi, s->fp32, cTW[a], cM, cP, 8);
+         nc[a] = sweep_candidates((int) nn[a], (int) (128 / s->esz_psi), (int) s->esz_psi, cTW[a], cM, cP, 8);
       const int ncmax = std::max(nc[0], std::max(nc[1], nc[2]));
       for (int c = 0; c < ncmax && st == GPE_OK; c++)
          for (int S = 2; S <= 3 && st == GPE_OK; S++) {

@@ -337,23 +337,6 @@ __device__ __forceinline__ void nu_pass_fp64(typename Tr<R, CPLX>::P *tile, cons
    }
 }
 
-// FP64 real-time calcnu applied as the x sweep's recurrence reads each point
-// (the arithmetic of nu_pass_fp64's real-time branch, so the result is the
-// same): no separate pass over the tile and no barrier after it, for the two
-// extra evaluations of the points above each segment.
-struct NuPhase64 {
-   const double *ptile;  // phi tile, row stride tw
-   int tw;
-   const double2 *ex;    // exp(-i dt V_x) along the line (shared memory)
-   double2 eyz;          // exp(-i dt (V_y + V_z)) of this column
-   double scale, g, gd, dt, invN;
-   template <class P> __device__ __forceinline__ P operator()(P v, int i) const {
-      const double2 p = scl(v, scale);
-      const double thn = dt * fma(fma(p.x, p.x, p.y * p.y), g, (ptile[i * tw] * invN) * gd);
-      return cmul(p, cmul(cmul(ex[i], eyz), expi_small(thn)));
-   }
-};
-
 // calcnu of the mixed-precision x sweep, applied as the sweep's recurrence
 // reads each point (measured faster than a separate pass over the tile in
 // FP32; slower in FP64, where a thread's extra evaluations for the two points
@@ -420,13 +403,11 @@ __device__ __forceinline__ NuTrap32<CPLX> nu_reads_fp32(const float *ptile_c, in
 // stores tile i-1 from the previous one.  Thread 0 issues every copy; before
 // refilling a stage it waits until the bulk store that last read the stage
 // has finished reading (all but the newest S-2 store groups).
-// Resident CTAs per SM the sweep kernels are compiled for (their register
-// budget): FP64 sweeps 2 (128 registers; three CTAs, 80 registers, spill the
-// 16-point segments and measured slower on B200); FP32 sweeps 4 (64
-// registers, 8- and 16-point segments fit without spills: twice the warps
-// per SM of the FP64 budget), the FP32 x sweep with its fused calcnu 3.  The
-// host never launches more per SM.
-template <class R> constexpr int sweep_ctas(bool nu) { return sizeof(R) == 8 ? 2 : (nu ? 3 : 4); }
+// Resident CTAs per SM the sweep kernels are compiled for (register
+// budget): [0] plain sweeps, [1] the x sweep fused with calcnu, whose tile
+// also stages phi.  The host never launches more per SM.  Three CTAs (80
+// registers) spill the 16-point segments and measured slower on B200.
+constexpr int kSweepCtas[2] = {2, 2};
 
 template <int S> __device__ __forceinline__ void wait_stage_free() {
    if constexpr (S == 2) bulk_wait_read<0>();
@@ -439,7 +420,7 @@ template <int S> __device__ __forceinline__ void wait_stage_free() {
 // With NU the x sweep first applies the pending 1/norm and calcnu to the tile
 // (needs phi).
 template <class R, bool CPLX, int AXIS, bool NU, int MSEG, int S, int TWC>
-__global__ void __launch_bounds__(256, sweep_ctas<R>(NU)) k_sweep_xy(const __grid_constant__ CUtensorMap tm_psi,
+__global__ void __launch_bounds__(256, kSweepCtas[NU ? 1 : 0]) k_sweep_xy(const __grid_constant__ CUtensorMap tm_psi,
                                                      const __grid_constant__ CUtensorMap tm_phi, Dims d, SegTab tb,
                                                      Trap trap, LinPhase lin, double g, double gd, double dt,
                                                      const State *__restrict__ st, int tw_arg, int boxn, int nbox,
@@ -513,19 +494,12 @@ __global__ void __launch_bounds__(256, sweep_ctas<R>(NU)) k_sweep_xy(const __gri
       if (__syncthreads_or(!mbar_wait(&full[q], (i / S) & 1, err))) break;
       P *tile = (P *) (base + q * stage_bytes);
       const int other = t / nzb, z0 = (t - other * nzb) * TW;
-      if constexpr (NU && std::is_same<R, double>::value && !CPLX) {
+      if constexpr (NU && std::is_same<R, double>::value) {
          nu_pass_fp64<R, CPLX, AXIS>(tile, (const R *) (tile + rows * TW), n, lg, c, other, z0, d, trap, lin, xtab, g,
                                      gd, dt, scale);
          __syncthreads();
       }
-      if constexpr (NU && std::is_same<R, double>::value && CPLX) {
-         static_assert(AXIS == 0, "calcnu is fused into the x sweep only");
-         const int k = min(z0 + c, d.nz - 1);  // columns past nz are zero fill, never stored
-         const NuPhase64 xf{(const double *) (tile + rows * TW) + c, TW, (const double2 *) xtab,
-                            cmul(__ldg((const double2 *) lin.ey + other), __ldg((const double2 *) lin.ez + k)), scale,
-                            g, gd, dt, 1.0 / (double) d.npts};
-         seg_sweep<R, CPLX, MSEG, TWC>(tile, TW, 1, c, p, TW, tb, blk, nullptr, nullptr, nullptr, nullptr, xf);
-      } else if constexpr (NU && std::is_same<R, float>::value) {
+      if constexpr (NU && std::is_same<R, float>::value) {
          static_assert(AXIS == 0, "calcnu is fused into the x sweep only");
          const NuTrap32<CPLX> xf = nu_reads_fp32<CPLX>((const float *) (tile + rows * TW) + c, TW, other, z0, c, d,
                                                        trap, lin, g, gd, dt, scale);
@@ -582,7 +556,7 @@ __device__ __forceinline__ void zsweep_tile(typename Tr<R, CPLX>::P *tile, int n
 // (rowsum2), the row partials of calcrms, so an rms sample after the step
 // needs no extra pass over psi.
 template <class R, bool CPLX, int MOM, int MSEG, int S, int TWC>
-__global__ void __launch_bounds__(256, sweep_ctas<R>(false)) k_sweep_z(typename Tr<R, CPLX>::P *__restrict__ psi, Dims d, SegTab tb,
+__global__ void __launch_bounds__(256, kSweepCtas[0]) k_sweep_z(typename Tr<R, CPLX>::P *__restrict__ psi, Dims d, SegTab tb,
                                                     int tr_arg, int LS, const double *__restrict__ wz,
                                                     const double *__restrict__ wz2, double hz3,
                                                     double *__restrict__ rowsum, double *__restrict__ rowsum2,
