@@ -461,29 +461,69 @@ extern "C" gpe_status gpe_batch_set_couplings(gpe_batch *b, const double *g, con
    return GPE_OK;
 }
 
+// Milliseconds per batch step with the instances' tiles as they are now: the
+// step is captured for them, one untimed step, then the best of two runs of
+// nsteps steps.
+static gpe_status time_batch(gpe_batch *b, int nsteps, double *ms) {
+   drop_tables(b);
+   double t = 0., best = 1e30;
+   BCKS(gpe_batch_time_steps(b, 1, &t));
+   for (int r = 0; r < 2; r++) {
+      BCKS(gpe_batch_time_steps(b, nsteps, &t));
+      best = std::min(best, t / nsteps);
+   }
+   *ms = best;
+   return GPE_OK;
+}
+
 extern "C" gpe_status gpe_batch_autotune(gpe_batch *b, int nsteps) {
    if (!b) return bfail(GPE_ERR_PARAM, "batch: null handle");
-   drop_tables(b);
+   if (nsteps < 1) return bfail(GPE_ERR_PARAM, "batch autotune needs nsteps >= 1");
+   BCK(cudaSetDevice(b->dev));
+   const size_t n = b->inst.size();
+   // every instance's psi and step state, put back at the end
+   std::vector<gpe::Stash> keep(n);
+   std::vector<gpe_tuning> start(n);
+   gpe_status st = GPE_OK;
+   for (size_t i = 0; i < n && st == GPE_OK; i++) {
+      st = gpe::tuning_as_set(b->inst[i], &start[i]);
+      if (st == GPE_OK) st = gpe::stash_take(b->inst[i], &keep[i]);
+   }
+   // the batch step with the tiles the instances start from
+   double t_start = 0., t_tuned = 0.;
+   if (st == GPE_OK) st = time_batch(b, nsteps, &t_start);
    // one autotuned representative per (grid, mode, precision)
    std::map<std::tuple<long, long, long, int, int>, gpe_tuning> done;
-   for (size_t i = 0; i < b->inst.size(); i++) {
+   for (size_t i = 0; i < n && st == GPE_OK; i++) {
       gpe_params p;
       gpe_solver *s = b->inst[i];
-      gpe_status st = gpe::params_of(s, &p);
-      if (st != GPE_OK) return st;
+      st = gpe::params_of(s, &p);
+      if (st != GPE_OK) break;
       const auto key = std::make_tuple(p.nx, p.ny, p.nz, p.mode, p.precision);
       auto it = done.find(key);
       if (it == done.end()) {
          gpe_tuning best;
          st = gpe_autotune(s, b->g[i], b->gd[i], nsteps, &best);
-         if (st != GPE_OK) return st;
-         done[key] = best;
+         if (st == GPE_OK) done[key] = best;
       } else {
          st = gpe_set_tuning(s, &it->second);
-         if (st != GPE_OK) return st;
       }
    }
-   return GPE_OK;
+   // a tile that is fastest for one instance's own launches need not be for
+   // the batched launches (one grid over all instances of a group, with other
+   // occupancy): the per-grid choices stay only if the batch step is faster
+   if (st == GPE_OK) st = time_batch(b, nsteps, &t_tuned);
+   if (st != GPE_OK || t_tuned >= t_start)
+      for (size_t i = 0; i < n; i++) {
+         gpe_status s2 = gpe_set_tuning(b->inst[i], &start[i]);
+         if (st == GPE_OK) st = s2;
+      }
+   drop_tables(b);
+   for (size_t i = 0; i < n; i++) {
+      gpe_status s2 = keep[i].psi ? gpe::stash_restore(b->inst[i], &keep[i]) : GPE_OK;
+      if (st == GPE_OK) st = s2;
+   }
+   return st;
 }
 
 extern "C" gpe_status gpe_batch_run(gpe_batch *b, long nsteps) {

@@ -25,6 +25,9 @@ cudaStream_t stream_of(gpe_solver *s);
 gpe_status params_of(gpe_solver *s, gpe_params *p);
 int device_of(gpe_solver *s);
 long long kernels_per_step(gpe_solver *s);
+// The tile choices as set (zeros where the planner picks): gpe_set_tuning
+// with them re-plans the handle exactly as before.
+gpe_status tuning_as_set(gpe_solver *s, gpe_tuning *t);
 
 // Batched launches (batch.cu): the instance's launch geometry under the
 // batch's tile choices with y / x FFT tiles of Ly / Lx columns (Ly = Lx = 0:
@@ -45,5 +48,18 @@ gpe_status batch_view_set(gpe_batch *b, const std::vector<gpe_solver *> &inst, c
 gpe_status batch_view_queue(gpe_batch *b, long nsteps);
 gpe_status batch_geom(gpe_solver *s, int Ly, int Lx, BatchGeom *geom);
 gpe_status batch_desc(gpe_solver *s, int Ly, int Lx, double g, double gd, BatchDesc *out);
+
+// A device copy of psi and a host copy of the step state (pending
+// renormalisation, couplings): stash_take makes it (one cudaMalloc, after the
+// handle's queued work), stash_restore writes it back and frees the copy,
+// stash_drop frees it without writing back.  Trial steps run in between.
+struct Stash {
+   void *psi = nullptr;
+   size_t bytes = 0;
+   unsigned char state[64];
+};
+gpe_status stash_take(gpe_solver *s, Stash *k);
+gpe_status stash_restore(gpe_solver *s, Stash *k);
+void stash_drop(Stash *k);
 
 }  // namespace gpe

@@ -1748,18 +1748,8 @@ extern "C" gpe_status gpe_autotune(gpe_solver *s, double g, double gd, int nstep
    CHECK_HANDLE(s);
    if (nsteps < 1) return fail(GPE_ERR_PARAM, "autotune needs nsteps >= 1");
    CK(cudaSetDevice(s->dev));
-   // keep psi and the step state
-   const size_t pbytes = s->esz_psi * (size_t) s->d.npts;
-   void *save = nullptr;
-   CK(cudaMalloc(&save, pbytes));
-   State st_save;
-   cudaError_t e = cudaMemcpyAsync(save, s->psi, pbytes, cudaMemcpyDeviceToDevice, s->st);
-   if (e == cudaSuccess) e = cudaMemcpyAsync(&st_save, s->state, sizeof(State), cudaMemcpyDeviceToHost, s->st);
-   if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
-   if (e != cudaSuccess) {
-      cudaFree(save);
-      return fail(GPE_ERR_CUDA, cudaGetErrorString(e));
-   }
+   gpe::Stash keep;  // psi and the step state, put back at the end
+   CKS(gpe::stash_take(s, &keep));
    const gpe_tuning start = s->tune;
    gpe_tuning pick = start;
    double best_sweep[3] = {1e30, 1e30, 1e30}, best_y = 1e30, best_x = 1e30, best_fft = 1e30;
@@ -1816,13 +1806,10 @@ extern "C" gpe_status gpe_autotune(gpe_solver *s, double g, double gd, int nstep
    }
    s->tune = st == GPE_OK ? pick : start;
    gpe_status st2 = plan_tiles(s);
-   e = cudaMemcpyAsync(s->psi, save, pbytes, cudaMemcpyDeviceToDevice, s->st);
-   if (e == cudaSuccess) e = cudaMemcpyAsync(s->state, &st_save, sizeof(State), cudaMemcpyHostToDevice, s->st);
-   if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
-   cudaFree(save);
+   gpe_status st3 = gpe::stash_restore(s, &keep);
    if (st != GPE_OK) return st;
    if (st2 != GPE_OK) return st2;
-   if (e != cudaSuccess) return fail(GPE_ERR_CUDA, cudaGetErrorString(e));
+   if (st3 != GPE_OK) return st3;
    if (best) *best = s->tune;
    return GPE_OK;
 }
@@ -1865,6 +1852,11 @@ gpe_status params_of(gpe_solver *s, gpe_params *p) {
 }
 int device_of(gpe_solver *s) { return s->dev; }
 long long kernels_per_step(gpe_solver *s) { return s->cplx ? 9 : 10; }
+gpe_status tuning_as_set(gpe_solver *s, gpe_tuning *t) {
+   CHECK_HANDLE(s);
+   *t = s->tune;
+   return GPE_OK;
+}
 
 gpe_status batch_geom(gpe_solver *s, int Ly, int Lx, BatchGeom *geom) {
    CHECK_HANDLE(s);
@@ -1874,6 +1866,41 @@ gpe_status batch_geom(gpe_solver *s, int Ly, int Lx, BatchGeom *geom) {
 gpe_status batch_desc(gpe_solver *s, int Ly, int Lx, double g, double gd, BatchDesc *out) {
    CHECK_HANDLE(s);
    return DISPATCH(s, desc(s, Ly, Lx, g, gd, out));
+}
+
+static_assert(sizeof(State) <= sizeof(Stash::state), "step state larger than its stash");
+
+gpe_status stash_take(gpe_solver *s, Stash *k) {
+   CHECK_HANDLE(s);
+   if (!k || k->psi) return fail(GPE_ERR_PARAM, "stash: null or already holding a copy");
+   CK(cudaSetDevice(s->dev));
+   k->bytes = s->esz_psi * (size_t) s->d.npts;
+   CK(cudaMalloc(&k->psi, k->bytes));
+   cudaError_t e = cudaMemcpyAsync(k->psi, s->psi, k->bytes, cudaMemcpyDeviceToDevice, s->st);
+   if (e == cudaSuccess) e = cudaMemcpyAsync(k->state, s->state, sizeof(State), cudaMemcpyDeviceToHost, s->st);
+   if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+   if (e != cudaSuccess) {
+      stash_drop(k);
+      return fail(GPE_ERR_CUDA, cudaGetErrorString(e));
+   }
+   return GPE_OK;
+}
+
+gpe_status stash_restore(gpe_solver *s, Stash *k) {
+   CHECK_HANDLE(s);
+   if (!k || !k->psi) return fail(GPE_ERR_PARAM, "stash: nothing to restore");
+   CK(cudaSetDevice(s->dev));
+   cudaError_t e = cudaMemcpyAsync(s->psi, k->psi, k->bytes, cudaMemcpyDeviceToDevice, s->st);
+   if (e == cudaSuccess) e = cudaMemcpyAsync(s->state, k->state, sizeof(State), cudaMemcpyHostToDevice, s->st);
+   if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+   stash_drop(k);
+   if (e != cudaSuccess) return fail(GPE_ERR_CUDA, cudaGetErrorString(e));
+   return GPE_OK;
+}
+
+void stash_drop(Stash *k) {
+   if (k && k->psi) cudaFree(k->psi);
+   if (k) k->psi = nullptr;
 }
 
 }  // namespace gpe

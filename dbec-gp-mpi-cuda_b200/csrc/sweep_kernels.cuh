@@ -402,18 +402,14 @@ __device__ __forceinline__ NuTrap32<CPLX> nu_reads_fp32(const float *ptile_c, in
 // tile i, the TMA engine already loads tile i+1 into the next stage and
 // stores tile i-1 from the previous one.  Thread 0 issues every copy; before
 // refilling a stage it waits until the bulk store that last read the stage
-// has finished reading (all but the newest S-2 store groups).
+// has finished reading (all but the newest S-2 store groups: wait_stage_free).
+//
 // Resident CTAs per SM the sweep kernels are compiled for (register
 // budget): [0] plain sweeps, [1] the x sweep fused with calcnu, whose tile
 // also stages phi.  The host never launches more per SM.  Three CTAs (80
 // registers) spill the 16-point segments and measured slower on B200.
 constexpr int kSweepCtas[2] = {2, 2};
 
-template <int S> __device__ __forceinline__ void wait_stage_free() {
-   if constexpr (S == 2) bulk_wait_read<0>();
-   else if constexpr (S == 3) bulk_wait_read<1>();
-   else bulk_wait_read<2>();
-}
 
 // x or y sweep.  Tile: TW consecutive z columns of one y (x sweep) or one x
 // (y sweep) plane, the whole line along the swept axis, brought in by TMA.

@@ -135,5 +135,12 @@ __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wa
 template <int N> __device__ __forceinline__ void bulk_wait_read() {
    asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
 }
+// In an S-stage pipeline (one store group per tile): the stage about to be
+// reloaded has been read out by its store.
+template <int S> __device__ __forceinline__ void wait_stage_free() {
+   if constexpr (S == 2) bulk_wait_read<0>();
+   else if constexpr (S == 3) bulk_wait_read<1>();
+   else bulk_wait_read<2>();
+}
 
 }  // namespace gpe

@@ -199,7 +199,10 @@ gpe_status gpe_batch_solver(gpe_batch *b, int i, gpe_solver **s);
 /* New couplings for every instance (the step graph is captured again). */
 gpe_status gpe_batch_set_couplings(gpe_batch *b, const double *g, const double *gd);
 /* Autotunes one instance per distinct (grid, mode, precision) with
- * gpe_autotune (nsteps per trial) and applies its choice to the others. */
+ * gpe_autotune (nsteps per trial) and applies its choice to the others, then
+ * keeps those choices only if a timed batch step (best of two runs of nsteps)
+ * is faster with them than with the tiles the instances had before; psi and
+ * the step state of every instance are as before the call. */
 gpe_status gpe_batch_autotune(gpe_batch *b, int nsteps);
 /* nsteps batch steps, then the pending renormalisation of imaginary-time
  * instances; returns after the GPU finished. */

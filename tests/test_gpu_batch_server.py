@@ -141,6 +141,38 @@ def test_batch_groups_and_new_couplings_bitwise(gpe_lib):
     b.close()
 
 
+def test_batch_autotune_keeps_psi_and_steps_bitwise(gpe_lib):
+    """The batch autotuner (per-grid trials, then a timed batch step with and
+    without the per-grid choices) leaves every instance's psi and pending
+    renormalisation as they were; the batch then steps with whichever tiles
+    it kept exactly as solo handles with those tiles do."""
+    gpe = gpe_lib
+    ps = [params(gpe, 0, (48, 48, 48), prec=1), params(gpe, 0, (48, 48, 48), prec=1),
+          params(gpe, 0, (64, 64, 64), prec=0), params(gpe, 1, (48, 40, 32), dx=0.2, dt=4e-4, trap=(1., 1., 4.))]
+    g = [100., 60., 80., 50.]
+    gd = [30., 20., 10., 5.]
+    b = gpe.Batch(ps, g, gd)
+    for i, p in enumerate(ps):
+        s = b.solver(i)
+        s.init_gaussian()
+        if p.mode == 0:
+            s.calcnorm(True)
+    b.run(3)
+    before = [b.solver(i).get_psi() for i in range(len(ps))]
+    b.autotune(1)
+    for i in range(len(ps)):
+        assert np.array_equal(b.solver(i).get_psi(), before[i]), i
+    b.run(4)
+    for i, p in enumerate(ps):
+        s = gpe.Solver(p)
+        s.set_tuning(b.solver(i).get_tuning())
+        s.set_psi(before[i])
+        s.run(4, g[i], gd[i])
+        assert np.array_equal(s.get_psi(), b.solver(i).get_psi()), i
+        s.close()
+    b.close()
+
+
 def _ground(gpe, shape, g, gd):
     return dict(params=params(gpe, 0, shape), kind=gpe.REQ_GROUND, g=g, gd=gd, tol=1e-6, check_every=50,
                 max_steps=3000)
