@@ -167,7 +167,10 @@ gpe_status build_tables(gpe_batch *b) {
          size_t sm = 128 + 2 * (size_t) A.stage[a] + A.blk[a] + A.extra[a];
          if (a == 2) sm += 2 * (size_t) A.part;
          if (sm > kSmemCap) return bfail(GPE_ERR_PARAM, "batch: sweep tiles exceed shared memory");
-         const int cap = a == 0 ? kSweepCtas[1] : kSweepCtas[0];
+         // the kernels' register budget holds kSweepCtas CTAs of 256 threads,
+         // so more of fewer threads
+         const int cap0 = a == 0 ? kSweepCtas[1] : kSweepCtas[0];
+         const int cap = std::max(1, std::min(32, 256 * cap0 / std::max(32, (int) A.threads[kPXsweep + a])));
          const int ctas = std::max(1, std::min(cap, (int) (kSmemCap / sm)));
          G.sweep_smem[a] = sm;
          G.sweep_grid[a] = (int) std::min<long long>(A.tiles[kPXsweep + a], (long long) ctas * b->nsm);
@@ -362,6 +365,15 @@ extern "C" gpe_status gpe_batch_create(const gpe_params *params, const double *g
       gpe_solver *s = nullptr;
       st = gpe_create(&params[i], nullptr, &s);
       if (st == GPE_OK) b->inst.push_back(s);
+      // mixed-precision imaginary time: 32-point segments in the y and z
+      // sweeps (fewer threads per tile, more CTAs per SM in the batched
+      // launches: 64-instance batch 1.95 -> 1.83 ms on B200; solo the small
+      // grids measured slower with them, so this is the batch's default only)
+      if (st == GPE_OK && params[i].mode == GPE_MODE_IMAG && params[i].precision == GPE_PREC_MIXED) {
+         gpe_tuning t{};
+         t.sweep_seg[1] = t.sweep_seg[2] = 32;
+         st = gpe_set_tuning(s, &t);
+      }
    }
    cudaError_t e = cudaSuccess;
    if (st == GPE_OK) {

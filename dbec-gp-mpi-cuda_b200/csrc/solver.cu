@@ -363,22 +363,34 @@ static gpe_status make_tmap(CUtensorMap *m, void *base, size_t esz, long w_nz, l
    return GPE_OK;
 }
 
-// Candidate (lines per CTA TW, segment length MSEG, segments P) for a sweep
+// Candidates (lines per CTA TW, segment length MSEG, segments P) for a sweep
 // over lines of length n, widest tile first: TW from `tw_base` (a 128-byte
-// row) down to 2, at most 256 threads (TW * P).  Lines of 16-byte elements
+// row) down to 2, and for each TW every segment length with at most 256
+// threads (TW * P), shortest first; prim[c] marks the shortest segment of
+// each TW (the most threads), the built-in choice.  Lines of 16-byte elements
 // keep 8-point segments (16 would spill registers); 4-byte elements may use
 // 32-point segments, which keep 64-byte tile rows on 512-point lines.
-static int sweep_candidates(int n, int tw_base, int esz, int *TW, int *MSEG, int *P, int cap) {
+constexpr int kSweepCand = 16;
+static int sweep_candidates(int n, int tw_base, int esz, int *TW, int *MSEG, int *P, bool *prim) {
    const bool wide = esz == 16;
    const int ms[3] = {8, 16, 32};
    const int nms = wide ? 1 : (esz == 4 ? 3 : 2);
    int k = 0;
-   for (int tw = tw_base; tw >= 2 && k < cap; tw /= 2)
-      for (int mi = 0; mi < nms && k < cap; mi++) {
+   for (int tw = tw_base; tw >= 2 && k < kSweepCand; tw /= 2) {
+      bool first = true;
+      for (int mi = 0; mi < nms && k < kSweepCand; mi++) {
          const int p = (n - 2 + ms[mi] - 1) / ms[mi];
-         if (tw * p <= 256) { TW[k] = tw; MSEG[k] = ms[mi]; P[k] = p; k++; break; }
+         if (tw * p <= 256) {
+            TW[k] = tw; MSEG[k] = ms[mi]; P[k] = p; prim[k] = first;
+            first = false;
+            k++;
+         }
       }
-   if (k == 0) { TW[0] = 2; MSEG[0] = wide ? 8 : 16; P[0] = (n - 2 + MSEG[0] - 1) / MSEG[0]; k = 1; }
+   }
+   if (k == 0) {
+      TW[0] = 2; MSEG[0] = wide ? 8 : 16; P[0] = (n - 2 + MSEG[0] - 1) / MSEG[0]; prim[0] = true;
+      k = 1;
+   }
    return k;
 }
 
@@ -398,8 +410,9 @@ static gpe_status plan_tiles(gpe_solver *s) {
       // the widest tile for which as many CTAs as the kernels are compiled for
       // fit on an SM with a 2-stage pipeline (else the widest tile, fewer CTAs)
       const int max_ctas = kSweepCtas[ax == 0 ? 1 : 0];
-      int cTW[8], cM[8], cP[8];
-      const int nc = sweep_candidates((int) nn[ax], tw_base, (int) esz, cTW, cM, cP, 8);
+      int cTW[kSweepCand], cM[kSweepCand], cP[kSweepCand];
+      bool prim[kSweepCand];
+      const int nc = sweep_candidates((int) nn[ax], tw_base, (int) esz, cTW, cM, cP, prim);
       auto sizes = [&](int TW, int P, size_t &stage, size_t &fixed) {
          const int spw = 32 / TW;
          const size_t blk = 2 * (size_t) ((P + spw - 1) / spw + 1) * TW * esz;
@@ -415,18 +428,34 @@ static gpe_status plan_tiles(gpe_solver *s) {
                     (s->fp32 ? 0 : 4 * (size_t) nn[2] * (s->cplx ? 16 : 8));
          }
       };
-      int pick = 0;
-      if (s->tune.sweep_tw[ax] > 0) {
-         pick = -1;
-         for (int c = 0; c < nc; c++)
-            if (cTW[c] == s->tune.sweep_tw[ax]) pick = c;
-         if (pick < 0) return fail(GPE_ERR_PARAM, "tuning: sweep_tw not available for this line length");
+      auto fits = [&](int c) {
+         size_t st_, fx_;
+         sizes(cTW[c], cP[c], st_, fx_);
+         return (fx_ + 2 * st_) * max_ctas <= sm_cap;
+      };
+      const int want_tw = s->tune.sweep_tw[ax], want_ms = s->tune.sweep_seg[ax];
+      // a candidate matching the fields that are set (an unset segment
+      // length means the shortest of that TW; an unset TW the widest tile
+      // that fits, else the widest)
+      auto match = [&](int c) { return (want_tw <= 0 || cTW[c] == want_tw) && (want_ms <= 0 ? prim[c] : cM[c] == want_ms); };
+      int pick = -1;
+      if (want_tw > 0 || want_ms > 0) {
+         for (int c = 0; c < nc && pick < 0; c++)
+            if (match(c) && (want_tw > 0 || fits(c))) pick = c;
+         for (int c = 0; c < nc && pick < 0; c++)
+            if (match(c)) pick = c;
+         if (pick < 0) return fail(GPE_ERR_PARAM, "tuning: sweep_tw / sweep_seg not available for this line length");
       } else {
-         for (int c = 0; c < nc; c++) {
-            size_t st_, fx_;
-            sizes(cTW[c], cP[c], st_, fx_);
-            if ((fx_ + 2 * st_) * max_ctas <= sm_cap) { pick = c; break; }
-         }
+         // FP32 real z lines of 100 points or more: 32-point segments when
+         // that leaves at least four per line (128^3 z sweep 20.1 -> 16.6 us
+         // on B200; shorter lines, and the x and y sweeps, measured no faster
+         // or slower with them solo)
+         if (ax == 2 && esz == 4)
+            for (int c = 0; c < nc && pick < 0; c++)
+               if (cM[c] == 32 && cP[c] >= 4 && fits(c)) pick = c;
+         for (int c = 0; c < nc && pick < 0; c++)
+            if (prim[c] && fits(c)) pick = c;
+         if (pick < 0) pick = 0;
       }
       w.TW = cTW[pick];
       w.MSEG = cM[pick];
@@ -1712,6 +1741,7 @@ extern "C" gpe_status gpe_get_tuning(gpe_solver *s, gpe_tuning *t) {
    for (int a = 0; a < 3; a++) {
       t->sweep_tw[a] = s->sw[a].TW;
       t->sweep_stages[a] = s->sw[a].S;
+      t->sweep_seg[a] = s->sw[a].MSEG;
    }
    t->fft_tile[0] = s->Ly;
    t->fft_tile[1] = s->Lx;
@@ -1755,18 +1785,22 @@ extern "C" gpe_status gpe_autotune(gpe_solver *s, double g, double gd, int nstep
    double best_sweep[3] = {1e30, 1e30, 1e30}, best_y = 1e30, best_x = 1e30, best_fft = 1e30;
    const int ksw[3] = {6, 7, 8};  // x, y, z sweeps in the kernel list
    gpe_status st = GPE_OK;
-   // sweeps: every available lines-per-CTA value with both pipeline depths
+   // sweeps: every available (lines per CTA, segment length) pair with both
+   // pipeline depths; the three axes are timed together, candidate c of
+   // each (its last one once an axis has fewer)
    {
       const long nn[3] = {s->d.nx, s->d.ny, s->d.nz};
-      int cTW[3][8], cM[8], cP[8], nc[3];
+      int cTW[3][kSweepCand], cM[3][kSweepCand], cP[kSweepCand], nc[3];
+      bool prim[kSweepCand];
       for (int a = 0; a < 3; a++)
-         nc[a] = sweep_candidates((int) nn[a], (int) (128 / s->esz_psi), (int) s->esz_psi, cTW[a], cM, cP, 8);
+         nc[a] = sweep_candidates((int) nn[a], (int) (128 / s->esz_psi), (int) s->esz_psi, cTW[a], cM[a], cP, prim);
       const int ncmax = std::max(nc[0], std::max(nc[1], nc[2]));
       for (int c = 0; c < ncmax && st == GPE_OK; c++)
          for (int S = 2; S <= 3 && st == GPE_OK; S++) {
             gpe_tuning t = start;
             for (int a = 0; a < 3; a++) {
                t.sweep_tw[a] = cTW[a][std::min(c, nc[a] - 1)];
+               t.sweep_seg[a] = cM[a][std::min(c, nc[a] - 1)];
                t.sweep_stages[a] = S;
             }
             s->tune = t;
@@ -1777,6 +1811,7 @@ extern "C" gpe_status gpe_autotune(gpe_solver *s, double g, double gd, int nstep
                if (ms[ksw[a]] < best_sweep[a]) {
                   best_sweep[a] = ms[ksw[a]];
                   pick.sweep_tw[a] = t.sweep_tw[a];
+                  pick.sweep_seg[a] = t.sweep_seg[a];
                   pick.sweep_stages[a] = S;
                }
          }

@@ -40,11 +40,12 @@ class Params(C.Structure):
 class Tuning(C.Structure):
     """gpe_tuning: tile configuration (0 = built-in heuristic)."""
     _fields_ = [("sweep_tw", C.c_int * 3), ("sweep_stages", C.c_int * 3), ("fft_tile", C.c_int * 2),
-                ("fft_max_radix", C.c_int)]
+                ("fft_max_radix", C.c_int), ("sweep_seg", C.c_int * 3)]
 
     def as_dict(self):
         return {"sweep_tw": list(self.sweep_tw), "sweep_stages": list(self.sweep_stages),
-                "fft_tile": list(self.fft_tile), "fft_max_radix": self.fft_max_radix}
+                "fft_tile": list(self.fft_tile), "fft_max_radix": self.fft_max_radix,
+                "sweep_seg": list(self.sweep_seg)}
 
 
 REQ_GROUND, REQ_EVOLVE = 0, 1

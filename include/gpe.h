@@ -156,6 +156,9 @@ typedef struct gpe_tuning {
    int sweep_stages[3]; /* TMA pipeline depth of the x, y, z sweeps: 2 or 3 */
    int fft_tile[2];     /* kz columns per tile of the y and x FFT passes */
    int fft_max_radix;   /* largest radix of the FFT plans: 16 (mixed precision only), 8, 4 or 2 */
+   int sweep_seg[3];    /* points per recurrence segment of the x, y, z sweeps: 8, 16 or
+                           32 (32: mixed-precision imaginary time only; complex FP64
+                           lines: 8) at most 256 threads per CTA */
 } gpe_tuning;
 /* The configuration in use (every field filled in). */
 gpe_status gpe_get_tuning(gpe_solver *s, gpe_tuning *t);
@@ -165,7 +168,7 @@ gpe_status gpe_get_tuning(gpe_solver *s, gpe_tuning *t);
 gpe_status gpe_set_tuning(gpe_solver *s, const gpe_tuning *t);
 /* Autotuner: times candidate configurations with gpe_profile_step (nsteps
  * steps each at couplings g, gd) and keeps, per sweep axis, the fastest lines
- * per CTA and pipeline depth, and for the FFT passes the fastest tile widths
+ * per CTA, segment length and pipeline depth, and for the FFT passes the fastest tile widths
  * and largest radix.  psi and the state are restored afterwards; the chosen
  * configuration is applied and returned in *best (may be NULL). */
 gpe_status gpe_autotune(gpe_solver *s, double g, double gd, int nsteps, gpe_tuning *best);
@@ -191,7 +194,10 @@ gpe_status gpe_snapshot_load(gpe_solver *s, const char *path, double *g, double 
  * CUDA graph with one branch per instance, are relaunched as one graph per
  * step, so small instances run concurrently on the GPU. */
 typedef struct gpe_batch gpe_batch;
-/* params[i] and couplings g[i], gd[i] of instance i (n >= 1). */
+/* params[i] and couplings g[i], gd[i] of instance i (n >= 1).  Instances in
+ * mixed-precision imaginary time start with 32-point segments in their y and z
+ * sweeps (gpe_tuning.sweep_seg), the batched launches' faster choice; any
+ * instance's tiles can be changed with gpe_set_tuning on its handle. */
 gpe_status gpe_batch_create(const gpe_params *params, const double *g, const double *gd, int n, gpe_batch **out);
 void gpe_batch_destroy(gpe_batch *b);
 /* The handle of instance i (owned by the batch): initial state, observables. */

@@ -1,10 +1,11 @@
 """Tile tuning, the batch runner and the request server (GPU).
 
 * tuning: another tile configuration gives the same step to rounding
-  (<= 1e-12 relative), a bad one is refused and the old one kept; the
-  autotuner leaves psi untouched;
-* batch: a batch step is exactly each instance's own step (bitwise equal to
-  running the instances one by one through gpe_run);
+  (<= 1e-12 relative in FP64, FP32 rounding for the segment length of the
+  mixed sweeps), a bad one is refused and the old one kept; the autotuners
+  (solo and batch) leave psi untouched;
+* batch: a batch step is exactly each instance's own step with the same tiles
+  (bitwise equal to running the instances one by one through gpe_run);
 * server: a ground-state request gives the same result (bitwise) whether it
   runs alone or among other requests, the HBM budget bounds the concurrent
   solves, and a request larger than the budget is refused with
@@ -56,6 +57,34 @@ def test_tuning_changes_only_rounding(gpe_lib):
     b.close()
 
 
+def test_segment_length_changes_only_rounding(gpe_lib):
+    """32-point recurrence segments (mixed-precision imaginary time) give the
+    step of the default 8/16-point segments to FP32 rounding; a segment length
+    a grid's elements do not have is refused."""
+    gpe = gpe_lib
+    p = params(gpe, 0, (128, 96, 128), dx=0.2, prec=1)
+    a, b = gpe.Solver(p), gpe.Solver(p)
+    assert list(a.get_tuning().sweep_seg)[1] == 16  # 96-point y lines: default 16
+    t = gpe.Tuning()
+    t.sweep_seg[0] = t.sweep_seg[1] = t.sweep_seg[2] = 32
+    b.set_tuning(t)
+    got = b.get_tuning()
+    assert list(got.sweep_seg) == [32, 32, 32] and all(v > 0 for v in got.sweep_tw)
+    for s in (a, b):
+        s.init_gaussian()
+        s.calcnorm(True)
+        s.run(20, 100., 30.)
+    assert rel(b.get_psi(), a.get_psi()) <= 1e-5  # FP32 rounding, 20 steps
+    f = gpe.Solver(params(gpe, 1, (32, 32, 32), dt=5e-4))
+    bad = gpe.Tuning()
+    bad.sweep_seg[2] = 32  # complex FP64 lines have 8-point segments only
+    with pytest.raises(gpe.GpeError) as e:
+        f.set_tuning(bad)
+    assert e.value.status == 1
+    for s in (a, b, f):
+        s.close()
+
+
 def test_autotune_keeps_psi(gpe_lib):
     gpe = gpe_lib
     s = gpe.Solver(params(gpe, 0, (64, 64, 64)))
@@ -94,6 +123,7 @@ def test_batch_equals_individual_runs(gpe_lib):
     assert b.launch_count() == 15 * (10 + 9)
     for i, p in enumerate(ps):
         s = gpe.Solver(p)
+        s.set_tuning(b.solver(i).get_tuning())
         s.init_gaussian()
         if p.mode == 0:
             s.calcnorm(True)
@@ -131,6 +161,7 @@ def test_batch_groups_and_new_couplings_bitwise(gpe_lib):
     b.run(5)
     for i, p in enumerate(ps):
         s = gpe.Solver(p)
+        s.set_tuning(b.solver(i).get_tuning())  # the batch's tiles (32-point segments in mixed imag time)
         s.init_gaussian()
         if p.mode == 0:
             s.calcnorm(True)
