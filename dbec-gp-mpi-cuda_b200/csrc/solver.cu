@@ -301,7 +301,9 @@ static gpe_status make_segtab(gpe_solver *s, int ax, long n, double d2, int m, i
    t.N = s->sw[ax].N;
    if (s->fp32) {
       // FP32 copies of the FP64 tables (alpha and gamma stay FP64 in HBM as
-      // computed; the FP32 kernels read these once-rounded copies)
+      // computed; the FP32 kernels read these once-rounded copies).  In real
+      // time the gamma copy holds gamma + 1 (SegOps::back_step): gamma is -1
+      // plus a small number, which FP32 keeps to its own relative precision.
       const void *src[4] = {s->alpha[ax], s->gamma[ax], s->sw[ax].M, s->sw[ax].N};
       const size_t nd = (size_t) n * (s->cplx ? 2 : 1);
       std::vector<double> h(nd);
@@ -310,7 +312,8 @@ static gpe_status make_segtab(gpe_solver *s, int ax, long n, double d2, int m, i
          if (s->sw[ax].t32[q]) cudaFree(s->sw[ax].t32[q]);
          s->sw[ax].t32[q] = nullptr;
          CK(cudaMemcpy(h.data(), src[q], sizeof(double) * nd, cudaMemcpyDeviceToHost));
-         for (size_t e = 0; e < nd; e++) f[e] = (float) h[e];
+         const bool shift = q == 1 && s->cplx;
+         for (size_t e = 0; e < nd; e++) f[e] = (float) (shift && e % 2 == 0 ? h[e] + 1. : h[e]);
          CKS(upload(&s->sw[ax].t32[q], f.data(), nd));
       }
       t.al = s->sw[ax].t32[0];

@@ -73,14 +73,30 @@ template <class R, bool CPLX> struct SegOps {
    //    t = 2 psi[i] - psi[i+1] - psi[i-1],
    // and gamma (A beta - r) = gamma (A (beta - t) - psi[i]).  `a` is A's
    // real (imag mode) or imaginary (real mode) part.
+   //
+   // FP32 real time: gamma = -1 / (A0 + A alpha) is -1 plus a small complex
+   // number (about i c), and a once-rounded FP32 gamma is off by up to half
+   // an FP32 ulp of 1 at every index, the same error at every step: the
+   // solve is then not unitary and the norm and mu drift linearly (1.7e-5
+   // and 5.7e-5 after 200 steps of a 32x30x40 test, the error of the whole
+   // mixed path; rounding alpha, A, psi, phi or the calcnu phase factor to
+   // FP32 instead changes mu by at most 2e-8 there, measured with the FP64
+   // oracle).  So the FP32 table holds gamma + 1, whose rounding error is
+   // that of the small part, and gamma u = (gamma + 1) u - u costs the same
+   // two multiply-adds per component.
    __device__ static P back_step(P b, P w2, P w1, P w0, P g, R a) {
       if constexpr (CPLX) {
          const R tx = fma((R) 2, w1.x, -w2.x) - w0.x, ty = fma((R) 2, w1.y, -w2.y) - w0.y;
          const R dx = b.x - tx, dy = b.y - ty;
          const R ux = fma(-a, dy, -w1.x), uy = fma(a, dx, -w1.y);
          P r;
-         r.x = fma(g.x, ux, -g.y * uy);
-         r.y = fma(g.x, uy, g.y * ux);
+         if constexpr (std::is_same<R, float>::value) {  // g = gamma + 1
+            r.x = fma(g.x, ux, fma(-g.y, uy, -ux));
+            r.y = fma(g.x, uy, fma(g.y, ux, -uy));
+         } else {
+            r.x = fma(g.x, ux, -g.y * uy);
+            r.y = fma(g.x, uy, g.y * ux);
+         }
          return r;
       } else {
          const R t = fma((R) 2, w1, -w2) - w0;
