@@ -16,8 +16,10 @@ every 100 steps.  A "step" is one full split step over the 256^3 grid
 The default line also carries the headline comparison of the metric
 (`baseline_metric`: the mixed-precision imaginary-time step at 256^3 against
 the plain FP64 step on the same box, with the mixed result's |dmu/mu| and
-density L2 error against the FP64 run after the same steps) and `cufft_ab`,
-the dipolar convolution timed through cuFFT against the solver's own passes.
+density L2 error against the FP64 run after the same steps), the same in real
+time on this workload (`baseline_metric_real_time`: complex64 against
+complex128) and `cufft_ab`, the dipolar convolution timed through cuFFT
+against the solver's own passes.
 --workload mixed256 prints that comparison as its own line;
 --workload mixed512 measures the mixed-precision imaginary-time step at
 512x512x256 instead (FP32 / complex64 bulk, FP64 reductions and tables);
@@ -476,6 +478,40 @@ def mixed_vs_plain(K, W, local, accuracy_steps):
             "meets_dmu_1e-6": abs(a["mu"] / b["mu"] - 1) <= 1e-6}
 
 
+def mixed_vs_plain_real(K, W, local, accuracy_steps):
+    """The same comparison in real time on this workload (real256: complex128
+    against complex64 at 256^3, gd = 80 after the quench): device-timed
+    grid-pt-steps/s of both steps, and the mixed result's error against the
+    FP64 run after `accuracy_steps` steps from the same Gaussian."""
+    import numpy as np
+    wl = WORKLOADS["real256"]
+    npts = int(np.prod(wl["grid"]))
+    G, GD = wl["g"], wl["gd"]
+    res = {}
+    for prec in (0, 1):
+        s, _ = make_solver(wl, local, precision=prec)
+        s.init_gaussian()
+        s.time_steps(W, G, GD)
+        ms = s.time_steps(K, G, GD)
+        s.init_gaussian()
+        s.run(accuracy_steps, G, GD)
+        mu, en = s.calcmuen(G, GD)
+        res[prec] = dict(ms=ms / K, value=npts * K / (ms / 1e3), mu=mu, en=en, norm=s.calcnorm(False),
+                         rms=s.calcrms(), rho=np.abs(s.get_psi()) ** 2)
+        s.close()
+    a, b = res[1], res[0]
+    den_l2 = float(np.linalg.norm((a["rho"] - b["rho"]).ravel()) / np.linalg.norm(b["rho"].ravel()))
+    return {"workload": "real256 in mixed precision (complex64 psi, FP32 FFT and sweeps, FP64 reductions and tables)",
+            "grid": list(wl["grid"]),
+            "mixed_grid_pt_steps_per_s": a["value"], "mixed_ms_per_step": a["ms"],
+            "plain_fp64_grid_pt_steps_per_s": b["value"], "plain_fp64_ms_per_step": b["ms"],
+            "vs_plain_fp64": a["value"] / b["value"],
+            "accuracy_steps": accuracy_steps, "dmu_rel": abs(a["mu"] / b["mu"] - 1),
+            "en_rel": abs(a["en"] / b["en"] - 1), "rms_rel": float(np.max(np.abs(a["rms"] - b["rms"]) / np.abs(b["rms"]))),
+            "norm_rel": abs(a["norm"] / b["norm"] - 1), "density_l2_rel": den_l2,
+            "meets_dmu_1e-6": abs(a["mu"] / b["mu"] - 1) <= 1e-6}
+
+
 def cufft_ab(wl, local, nrep=10):
     """The dipolar convolution of this workload through cuFFT (the reference's
     call structure, and one batched plan per direction) against the solver's
@@ -653,6 +689,8 @@ def main():
     if rank == 0 and world == 1:
         if args.workload in ("real256", "mixed256"):
             extra["baseline_metric"] = mixed_vs_plain(K, W, local, args.accuracy_steps)
+        if args.workload == "real256":
+            extra["baseline_metric_real_time"] = mixed_vs_plain_real(K, W, local, args.accuracy_steps)
         if args.workload in ("real256", "mixed512"):
             extra["cufft_ab"] = cufft_ab(wl, local)
 
