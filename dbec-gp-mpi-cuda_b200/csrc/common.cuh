@@ -21,6 +21,50 @@ template <class C> __host__ __device__ __forceinline__ C cmul(C a, C b) {
 }
 template <class C> __host__ __device__ __forceinline__ C cconj(C a) { C r; r.x = a.x; r.y = -a.y; return r; }
 template <class C, class S> __host__ __device__ __forceinline__ C cscale(C a, S s) { C r; r.x = a.x * s; r.y = a.y * s; return r; }
+// Complex float adds, subtracts and real scalings as one packed two-lane
+// FP32 instruction each on sm_100 (PTX add/sub/mul.rn.f32x2, each lane
+// rounded as the scalar instruction rounds it; the compiler no longer fuses
+// such a multiply with a following add, which moves FP32 results by a last
+// bit).  The FP32 FFT stages are mostly such adds and subtracts and are bound
+// by instruction issue.
+__device__ __forceinline__ unsigned long long f2_pack(float2 v) {
+   unsigned long long r;
+   asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(v.x), "f"(v.y));
+   return r;
+}
+__device__ __forceinline__ float2 f2_unpack(unsigned long long r) {
+   float2 v;
+   asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
+   return v;
+}
+__host__ __device__ __forceinline__ float2 cadd(float2 a, float2 b) {
+#ifdef __CUDA_ARCH__
+   unsigned long long r;
+   asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2_pack(a)), "l"(f2_pack(b)));
+   return f2_unpack(r);
+#else
+   return make_float2(a.x + b.x, a.y + b.y);
+#endif
+}
+__host__ __device__ __forceinline__ float2 csub(float2 a, float2 b) {
+#ifdef __CUDA_ARCH__
+   unsigned long long r;
+   asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2_pack(a)), "l"(f2_pack(b)));
+   return f2_unpack(r);
+#else
+   return make_float2(a.x - b.x, a.y - b.y);
+#endif
+}
+__host__ __device__ __forceinline__ float2 cscale(float2 a, float s) {
+#ifdef __CUDA_ARCH__
+   unsigned long long r;
+   asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2_pack(a)), "l"(f2_pack(make_float2(s, s))));
+   return f2_unpack(r);
+#else
+   return make_float2(a.x * s, a.y * s);
+#endif
+}
+
 // multiply by -i (forward) or +i (inverse)
 template <class C, bool INV> __host__ __device__ __forceinline__ C mul_mi(C a) {
    C r;
