@@ -25,8 +25,10 @@ template <class C, class S> __host__ __device__ __forceinline__ C cscale(C a, S 
 // FP32 instruction each on sm_100 (PTX add/sub/mul.rn.f32x2, each lane
 // rounded as the scalar instruction rounds it; the compiler no longer fuses
 // such a multiply with a following add, which moves FP32 results by a last
-// bit).  The FP32 FFT stages are mostly such adds and subtracts and are bound
-// by instruction issue.
+// bit), and a complex product as a packed multiply and a packed
+// multiply-add.  The FP32 FFT stages are mostly such operations and are
+// bound by instruction issue (mixed 256^3 step 0.439 -> 0.428 ms for the
+// adds, subtracts and scalings, 0.415 -> 0.411 ms for the products).
 __device__ __forceinline__ unsigned long long f2_pack(float2 v) {
    unsigned long long r;
    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(v.x), "f"(v.y));
@@ -62,6 +64,20 @@ __host__ __device__ __forceinline__ float2 cscale(float2 a, float s) {
    return f2_unpack(r);
 #else
    return make_float2(a.x * s, a.y * s);
+#endif
+}
+
+__host__ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+#ifdef __CUDA_ARCH__
+   // (a.x b.x, a.x b.y) + (-a.y b.y, a.y b.x)
+   unsigned long long t, r;
+   asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(t) : "l"(f2_pack(make_float2(a.x, a.x))), "l"(f2_pack(b)));
+   asm("fma.rn.f32x2 %0, %1, %2, %3;"
+       : "=l"(r)
+       : "l"(f2_pack(make_float2(-a.y, a.y))), "l"(f2_pack(make_float2(b.y, b.x))), "l"(t));
+   return f2_unpack(r);
+#else
+   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 #endif
 }
 
