@@ -509,10 +509,12 @@ static gpe_status plan_tiles(gpe_solver *s) {
       const long ppt = s->fp32 ? 16 : 8;  // FftL<R>::PPT
       // FP64 starts from 4 columns: on B200 the 128-thread CTAs of 4-column
       // tiles (eight per SM) measured faster than 8-column tiles (four per
-      // SM): y pass 60 -> 56 us, 256^3 step 0.870 -> 0.863 ms; FP32 widths
-      // measured alike
+      // SM): y pass 60 -> 56 us, 256^3 step 0.870 -> 0.863 ms.  FP32 starts
+      // from 8 columns (64-byte rows): mixed 256^3 step 0.412 -> 0.403 ms
+      // against 16 columns, 128^3 0.103 -> 0.102 ms, 512x512x256 (8 columns
+      // either way) unchanged
       auto pickL = [&](long rows) {
-         int L = s->fp32 ? 128 / (int) s->esz_c : 4;
+         int L = s->fp32 ? 8 : 4;
          while (L > 2 && rows * L > 256 * ppt) L /= 2;
          return L;
       };
@@ -1842,13 +1844,34 @@ extern "C" gpe_status gpe_autotune(gpe_solver *s, double g, double gd, int nstep
       const double f = ms[0] + ms[1] + ms[2] + ms[3] + ms[4];
       if (f < best_fft) { best_fft = f; pick.fft_max_radix = r; }
    }
+   // the per-kernel choices are combined: keep them only if whole steps
+   // (launched as a run launches them, each kernel overlapping the drain of
+   // the one before) are faster than with the configuration the tuner
+   // started from (on B200 the combined picks once made the mixed real-time
+   // step 13 % slower)
+   if (st == GPE_OK) {
+      double t_pick = 1e30, t_start = 1e30;
+      const gpe_tuning cand[2] = {pick, start};
+      double *tt[2] = {&t_pick, &t_start};
+      for (int k = 0; k < 2 && st == GPE_OK; k++) {
+         s->tune = cand[k];
+         st = plan_tiles(s);
+         double ms = 0.;
+         if (st == GPE_OK) st = gpe_time_steps(s, 1, g, gd, &ms);
+         for (int r = 0; r < 2 && st == GPE_OK; r++) {
+            st = gpe_time_steps(s, 2 * nsteps, g, gd, &ms);
+            *tt[k] = std::min(*tt[k], ms);
+         }
+      }
+      if (st == GPE_OK && t_pick >= t_start) pick = start;
+   }
    s->tune = st == GPE_OK ? pick : start;
    gpe_status st2 = plan_tiles(s);
    gpe_status st3 = gpe::stash_restore(s, &keep);
    if (st != GPE_OK) return st;
    if (st2 != GPE_OK) return st2;
    if (st3 != GPE_OK) return st3;
-   if (best) *best = s->tune;
+   if (best) return gpe_get_tuning(s, best);  // every field filled in
    return GPE_OK;
 }
 

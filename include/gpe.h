@@ -167,10 +167,13 @@ gpe_status gpe_get_tuning(gpe_solver *s, gpe_tuning *t);
  * fit this grid. */
 gpe_status gpe_set_tuning(gpe_solver *s, const gpe_tuning *t);
 /* Autotuner: times candidate configurations with gpe_profile_step (nsteps
- * steps each at couplings g, gd) and keeps, per sweep axis, the fastest lines
- * per CTA, segment length and pipeline depth, and for the FFT passes the fastest tile widths
- * and largest radix.  psi and the state are restored afterwards; the chosen
- * configuration is applied and returned in *best (may be NULL). */
+ * steps each at couplings g, gd) and picks, per sweep axis, the fastest lines
+ * per CTA, segment length and pipeline depth, and for the FFT passes the
+ * fastest tile widths and largest radix; the picks are kept only if whole
+ * steps (gpe_time_steps, best of two runs of 2 nsteps) are faster with them
+ * than with the configuration the call started from.  psi and the state are
+ * restored afterwards; the configuration in use is returned in *best (may be
+ * NULL). */
 gpe_status gpe_autotune(gpe_solver *s, double g, double gd, int nsteps, gpe_tuning *best);
 
 /* Snapshot of a solve (no reference counterpart: the reference's
