@@ -53,6 +53,7 @@ struct gpe_batch {
    cudaEvent_t fork = nullptr;
    std::vector<Group> groups;
    bool tables = false;  // groups and device tables built
+   std::vector<unsigned long long> gen;  // instances' plan generations the tables were built for
    cudaGraph_t graph = nullptr;
    cudaGraphExec_t exec = nullptr;
    long long kernels_per_step = 0;
@@ -95,6 +96,19 @@ void drop_tables(gpe_batch *b) {
    }
    b->groups.clear();
    b->tables = false;
+}
+
+// Tables (and the captured step) built before an instance's tiles were
+// planned again (gpe_set_tuning or gpe_autotune on its handle) are dropped,
+// so the next step rebuilds them: the old descriptors still point at the
+// instance's freed segment tables and carry its old tile geometry.
+void refresh(gpe_batch *b) {
+   if (!b->tables) return;
+   for (size_t i = 0; i < b->inst.size(); i++)
+      if (i >= b->gen.size() || gpe::plan_generation(b->inst[i]) != b->gen[i]) {
+         drop_tables(b);
+         return;
+      }
 }
 
 constexpr size_t kSmemCap = 227 * 1024;
@@ -192,6 +206,8 @@ gpe_status build_tables(gpe_batch *b) {
       BCK(cudaMemcpyAsync(G.dwork, work.data(), sizeof(unsigned) * work.size(), cudaMemcpyHostToDevice, b->master));
    }
    BCK(cudaStreamSynchronize(b->master));
+   b->gen.clear();
+   for (gpe_solver *s : b->inst) b->gen.push_back(gpe::plan_generation(s));
    b->tables = true;
    return GPE_OK;
 }
@@ -442,6 +458,7 @@ gpe_status batch_view_queue(gpe_batch *b, long nsteps) {
    if (!b || nsteps < 0) return bfail(GPE_ERR_PARAM, "batch view: null or negative step count");
    if (b->inst.empty() || nsteps == 0) return GPE_OK;
    BCK(cudaSetDevice(b->dev));
+   refresh(b);
    if (!b->exec) BCKS(capture(b));
    for (long c = 0; c < nsteps; c++) BCK(cudaGraphLaunch(b->exec, b->master));
    b->launches += b->kernels_per_step * nsteps;
@@ -460,6 +477,7 @@ extern "C" gpe_status gpe_batch_set_couplings(gpe_batch *b, const double *g, con
    if (!b || !g || !gd) return bfail(GPE_ERR_PARAM, "batch: null argument");
    b->g.assign(g, g + b->inst.size());
    b->gd.assign(gd, gd + b->inst.size());
+   refresh(b);
    if (!b->tables) return GPE_OK;
    // rewrite the descriptor tables in place, in stream order after any batch
    // step already queued; the captured graph reads them at run time
@@ -542,6 +560,7 @@ extern "C" gpe_status gpe_batch_run(gpe_batch *b, long nsteps) {
    if (!b || nsteps < 0) return bfail(GPE_ERR_PARAM, "batch: null handle or negative step count");
    BCK(cudaSetDevice(b->dev));
    if (nsteps == 0) return GPE_OK;
+   refresh(b);
    if (!b->exec) BCKS(capture(b));
    BCKS(fan_in(b));
    for (long c = 0; c < nsteps; c++) BCK(cudaGraphLaunch(b->exec, b->master));
@@ -556,6 +575,7 @@ extern "C" gpe_status gpe_batch_run(gpe_batch *b, long nsteps) {
 extern "C" gpe_status gpe_batch_time_steps(gpe_batch *b, long nsteps, double *ms) {
    if (!b || nsteps < 1) return bfail(GPE_ERR_PARAM, "batch: null handle or nsteps < 1");
    BCK(cudaSetDevice(b->dev));
+   refresh(b);
    if (!b->exec) BCKS(capture(b));
    BCKS(fan_in(b));
    cudaEvent_t e0, e1;
@@ -583,6 +603,7 @@ extern "C" gpe_status gpe_batch_profile_step(gpe_batch *b, long nsteps, double *
    if (!b || !ms || nsteps < 1) return bfail(GPE_ERR_PARAM, "batch: null argument or nsteps < 1");
    if (cap < kNPass) return bfail(GPE_ERR_PARAM, "batch: profile output array too small");
    BCK(cudaSetDevice(b->dev));
+   refresh(b);
    if (!b->tables) BCKS(build_tables(b));
    BCKS(fan_in(b));
    const size_t ng = b->groups.size();

@@ -25,6 +25,9 @@ cudaStream_t stream_of(gpe_solver *s);
 gpe_status params_of(gpe_solver *s, gpe_params *p);
 int device_of(gpe_solver *s);
 long long kernels_per_step(gpe_solver *s);
+// Counts the handle's tile plannings (gpe_set_tuning, gpe_autotune): a batch
+// compares it with the value its descriptors were built for.
+unsigned long long plan_generation(gpe_solver *s);
 // The tile choices as set (zeros where the planner picks): gpe_set_tuning
 // with them re-plans the handle exactly as before.
 gpe_status tuning_as_set(gpe_solver *s, gpe_tuning *t);

@@ -75,6 +75,9 @@ struct gpe_solver {
    int boxy = 0, nboxy = 1, boxx = 0, nboxx = 1;
    int Ly = 8, Lx = 8;  // kz columns per tile of the y and x passes
    gpe_tuning tune{};   // requested tile configuration (0 = default heuristic)
+   // bumped whenever the tiles are planned again (their tables reallocated):
+   // batches built over this handle rebuild their descriptors when it moves
+   unsigned long long plan_gen = 0;
    size_t esz_psi = 8, esz_c = 16, esz_r = 8;
    void *psi = nullptr, *spec = nullptr, *phi = nullptr;
    void *twx = nullptr, *twy = nullptr, *twz = nullptr;
@@ -401,6 +404,7 @@ static int sweep_candidates(int n, int tw_base, int esz, int *TW, int *MSEG, int
 // plans: the heuristics below, or the values of s->tune where set.  May be
 // called again (gpe_set_tuning); it reuploads only the segment tables.
 static gpe_status plan_tiles(gpe_solver *s) {
+   s->plan_gen++;
    const Dims &d = s->d;
    const size_t esz = s->esz_psi, rsz = s->esz_r;
    const int E = s->cplx ? 2 : 1;
@@ -1913,6 +1917,7 @@ gpe_status params_of(gpe_solver *s, gpe_params *p) {
 }
 int device_of(gpe_solver *s) { return s->dev; }
 long long kernels_per_step(gpe_solver *s) { return s->cplx ? 9 : 10; }
+unsigned long long plan_generation(gpe_solver *s) { return s->plan_gen; }
 gpe_status tuning_as_set(gpe_solver *s, gpe_tuning *t) {
    CHECK_HANDLE(s);
    *t = s->tune;

@@ -172,6 +172,44 @@ def test_batch_groups_and_new_couplings_bitwise(gpe_lib):
     b.close()
 
 
+def test_batch_follows_a_retuned_instance(gpe_lib):
+    """An instance re-planned through its own handle after the batch has
+    stepped (gpe_set_tuning) makes the batch rebuild its descriptors and
+    captured step: the next batch steps equal solo steps with the new tiles,
+    bit for bit."""
+    gpe = gpe_lib
+    ps = [params(gpe, 0, (64, 64, 64), prec=1), params(gpe, 0, (48, 48, 48), prec=1),
+          params(gpe, 1, (32, 32, 32), dt=5e-4)]
+    g, gd = [100., 60., 40.], [30., 20., 5.]
+    b = gpe.Batch(ps, g, gd)
+    first = [b.solver(i).get_tuning() for i in range(len(ps))]
+    for i, p in enumerate(ps):
+        s = b.solver(i)
+        s.init_gaussian()
+        if p.mode == 0:
+            s.calcnorm(True)
+    b.run(3)
+    t = gpe.Tuning()
+    t.sweep_tw[0] = 8
+    t.sweep_seg[1] = 16
+    t.fft_tile[0] = 4
+    b.solver(0).set_tuning(t)
+    b.run(4)
+    for i, p in enumerate(ps):
+        s = gpe.Solver(p)
+        s.set_tuning(first[i])
+        s.init_gaussian()
+        if p.mode == 0:
+            s.calcnorm(True)
+        s.run(3, g[i], gd[i])
+        if i == 0:
+            s.set_tuning(t)
+        s.run(4, g[i], gd[i])
+        assert np.array_equal(s.get_psi(), b.solver(i).get_psi()), i
+        s.close()
+    b.close()
+
+
 def test_batch_autotune_keeps_psi_and_steps_bitwise(gpe_lib):
     """The batch autotuner (per-grid trials, then a timed batch step with and
     without the per-grid choices) leaves every instance's psi and pending
