@@ -384,10 +384,14 @@ extern "C" gpe_status gpe_batch_create(const gpe_params *params, const double *g
       // mixed-precision imaginary time: 32-point segments in the y and z
       // sweeps (fewer threads per tile, more CTAs per SM in the batched
       // launches: 64-instance batch 1.95 -> 1.83 ms on B200; solo the small
-      // grids measured slower with them, so this is the batch's default only)
+      // grids measured slower with them, so this is the batch's default
+      // only), the z sweep on 16-row tiles with a 3-stage pipeline (1.758 ->
+      // 1.740 ms)
       if (st == GPE_OK && params[i].mode == GPE_MODE_IMAG && params[i].precision == GPE_PREC_MIXED) {
          gpe_tuning t{};
          t.sweep_seg[1] = t.sweep_seg[2] = 32;
+         t.sweep_tw[2] = 16;
+         t.sweep_stages[2] = 3;
          st = gpe_set_tuning(s, &t);
       }
    }

@@ -456,10 +456,15 @@ static gpe_status plan_tiles(gpe_solver *s) {
          // FP32 real z lines of 100 points or more: 32-point segments when
          // that leaves at least four per line (128^3 z sweep 20.1 -> 16.6 us
          // on B200; shorter lines, and the x and y sweeps, measured no faster
-         // or slower with them solo)
-         if (ax == 2 && esz == 4)
+         // or slower with them solo), on 16-row tiles where those fit (with
+         // a 3-stage pipeline, below: mixed 256^3 step 0.4117 -> 0.4088 ms,
+         // 512x512x256 1.676 -> 1.666 ms)
+         if (ax == 2 && esz == 4) {
+            for (int c = 0; c < nc && pick < 0; c++)
+               if (cM[c] == 32 && cP[c] >= 4 && cTW[c] == 16 && fits(c)) pick = c;
             for (int c = 0; c < nc && pick < 0; c++)
                if (cM[c] == 32 && cP[c] >= 4 && fits(c)) pick = c;
+         }
          for (int c = 0; c < nc && pick < 0; c++)
             if (prim[c] && fits(c)) pick = c;
          if (pick < 0) pick = 0;
@@ -487,7 +492,9 @@ static gpe_status plan_tiles(gpe_solver *s) {
       // default depth: 3 for the TMA tensor tiles of the x / y sweeps, 2 for
       // the z sweep's bulk-copied rows (measured faster on B200 at 256^3, both
       // modes)
-      const int s_hi = s->tune.sweep_stages[ax] > 0 ? s->tune.sweep_stages[ax] : (ax == 2 ? 2 : 3);
+      // (FP32 real z sweeps on 16-row tiles of 32-point segments: 3)
+      const bool z16 = ax == 2 && esz == 4 && w.TW == 16 && w.MSEG == 32;
+      const int s_hi = s->tune.sweep_stages[ax] > 0 ? s->tune.sweep_stages[ax] : ((ax == 2 && !z16) ? 2 : 3);
       const int s_lo = s->tune.sweep_stages[ax] > 0 ? s->tune.sweep_stages[ax] : 2;
       if (s_lo < 2 || s_hi > 3) return fail(GPE_ERR_PARAM, "tuning: sweep_stages must be 2 or 3");
       // the register budget of max_ctas CTAs of 256 threads holds more CTAs
