@@ -253,6 +253,9 @@ static gpe_status make_coef(gpe_solver *s, int ax, long n, double d2) {
 //   N[k] = prod_{j=lo_p}^{k-1} alpha[j]       for k in (lo_p, hf_p + 1]
 // computed in long double and rounded once.
 static gpe_status make_segtab(gpe_solver *s, int ax, long n, double d2, int m, int P) {
+   // the z sweep's Simpson partials take the weight of a point from its
+   // parity within the segment, so segments start at even indices
+   if (m % 2) return fail(GPE_ERR_PARAM, "segment length must be even");
    typedef std::complex<long double> Z;
    const long double c = (long double) s->p.dt / (long double) d2 / (3.L - (long double) s->par);
    Z A0, A;

@@ -122,9 +122,13 @@ template <class R, bool CPLX> struct SegOps {
 // t = p * TW + c owns recurrence indices [p m, hf] of line c.  A warp holds
 // SPW = 32 / TW consecutive segments of each of its TW lines.  blk is a
 // shared scratch of 2 * (NW + 1) * TW elements (NW warps hold segments).
-// Writes the swept line back in place.  When simp_w is non-null, *simp
-// receives this thread's share of sum_i simp_w[i] |psi'_i|^2, and when
-// simp_w2 is non-null *simp2 that of sum_i simp_w2[i] |psi'_i|^2.  Every
+// Writes the swept line back in place.  When simp_w and simp_w2 are
+// non-null, *simp receives this thread's share of sum_i simp_w[i] |psi'_i|^2
+// and *simp2 that of sum_i simp_w2[i] |psi'_i|^2.  When only simp_w is
+// non-null, *simp receives the share with the interior Simpson weights, 4 at
+// odd i and 2 at even i, applied by parity without reading the table (a
+// segment starts at an even index, m being even); the caller adds the end
+// correction of an even-length line (simp_w's other entries).  Every
 // value of the line the recurrence reads goes through xf(value, i) first
 // (the fused calcnu of the x sweep; identity otherwise); a thread reads its
 // own points and the two above its segment, so no transformed copy of the
@@ -242,7 +246,7 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
       bb[w * TW + c] = sb;
    }
    __syncthreads();
-   double acc = 0., acc2 = 0.;
+   double acc = 0., acc2 = 0., acc_o = 0., acc_e = 0.;
    {
       P x = zero_of<P>();  // psi' entering the first segment of this warp
       for (int ww = 0; ww < w; ww++) x = Op::fma_(ba[ww * TW + c], x, bb[ww * TW + c]);
@@ -258,8 +262,14 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
                line[k * es] = val;
                if (simp_w) {
                   const double f = (double) dens2(val);
-                  acc += simp_w[k] * f;
-                  if (simp_w2) acc2 += simp_w2[k] * f;
+                  if (simp_w2) {
+                     acc += simp_w[k] * f;
+                     acc2 += simp_w2[k] * f;
+                  } else if (q & 1) {  // k = lo + q + 1 even
+                     acc_e += f;
+                  } else {
+                     acc_o += f;
+                  }
                }
             }
          }
@@ -267,7 +277,7 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
          if (top) line[(n - 1) * es] = zero_of<P>();
       }
    }
-   if (simp) *simp = acc;
+   if (simp) *simp = simp_w2 ? acc : fma(4., acc_o, 2. * acc_e);
    if (simp2) *simp2 = acc2;
 }
 
@@ -549,14 +559,24 @@ __device__ __forceinline__ void zsweep_tile(typename Tr<R, CPLX>::P *tile, int n
    if (MOM == 2 && p < tbs.P) part2[p * TR + c] = my2;
    fence_proxy_async();
    __syncthreads();
-   if (SIMP && p == 0 && c < nr) {
+   // row rr's sums on the last warp, so that warp 0 (whose thread 0 issues
+   // the tile's store and the next load) goes on at once (TR <= 32)
+   const int rr = (int) threadIdx.x - ((int) blockDim.x - 32);
+   if (SIMP && rr >= 0 && rr < nr) {
       double sum = 0.;
-      for (int pp = 0; pp < tbs.P; pp++) sum += part[pp * TR + c];
-      rowsum[row0 + c] = sum * hz3;
+      for (int pp = 0; pp < tbs.P; pp++) sum += part[pp * TR + rr];
+      if (MOM == 1 && !(tbs.n & 1)) {
+         // the end correction of an even nz: the weights of points nz-2 and
+         // nz-3 are 3 and 3.75 where the interior weights give 2 and 4
+         const int n = tbs.n;
+         const typename Tr<R, CPLX>::P *row = tile + rr * LS;
+         sum += (double) dens2(row[n - 2]) - 0.25 * (double) dens2(row[n - 3]);
+      }
+      rowsum[row0 + rr] = sum * hz3;
       if (MOM == 2) {
          double sum2 = 0.;
-         for (int pp = 0; pp < tbs.P; pp++) sum2 += part2[pp * TR + c];
-         rowsum2[row0 + c] = sum2 * hz3;
+         for (int pp = 0; pp < tbs.P; pp++) sum2 += part2[pp * TR + rr];
+         rowsum2[row0 + rr] = sum2 * hz3;
       }
    }
 }
