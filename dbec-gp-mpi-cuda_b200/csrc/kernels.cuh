@@ -64,13 +64,29 @@ struct LinPhase {
 };
 
 // exp(t) for the nonlinear part of the step's exponent, which is small in
-// practice: Taylor series on |t| <= 0.5 (through t^16; the first omitted term
-// is below 2.2e-20 relative), the library function beyond.
+// practice: Taylor series on |t| <= 1/8 (through t^10; the first omitted
+// term is below 3e-18) and on |t| <= 0.5 (through t^16; below 2.2e-20
+// relative), the library function beyond.  The short series is the common
+// case: with it the 256^3 FP64 imaginary-time step (dt = 4e-3, g = 200)
+// measured 0.667 -> 0.663 ms on B200.
 __device__ __forceinline__ double exp_small(double t) {
    if (fabs(t) > 0.5) return exp(t);
    constexpr double f2 = 1. / 2, f3 = f2 / 3, f4 = f3 / 4, f5 = f4 / 5, f6 = f5 / 6, f7 = f6 / 7, f8 = f7 / 8,
                     f9 = f8 / 9, f10 = f9 / 10, f11 = f10 / 11, f12 = f11 / 12, f13 = f12 / 13, f14 = f13 / 14,
                     f15 = f14 / 15, f16 = f15 / 16;
+   if (fabs(t) <= 0.125) {
+      double e = f10;
+      e = fma(e, t, f9);
+      e = fma(e, t, f8);
+      e = fma(e, t, f7);
+      e = fma(e, t, f6);
+      e = fma(e, t, f5);
+      e = fma(e, t, f4);
+      e = fma(e, t, f3);
+      e = fma(e, t, f2);
+      e = fma(e, t, 1.);
+      return fma(e, t, 1.);
+   }
    double e = f16;
    e = fma(e, t, f15);
    e = fma(e, t, f14);
