@@ -282,9 +282,12 @@ __device__ __forceinline__ void seg_sweep(typename Tr<R, CPLX>::P *s, int es, in
 }
 
 // exp(-i t) = (cos t, -sin t) for the nonlinear part of the real-time phase,
-// which is small in practice: Maclaurin series on |t| <= 0.25 (through t^11
-// for sin and t^12 for cos; the first omitted terms are below 3e-18), the
-// library sincos beyond.
+// which is small in practice: Maclaurin series on |t| <= 1/32 (through t^7
+// for sin and t^6 for cos; the first omitted terms are below 3e-18 relative
+// to sin and 3e-17 to cos) and on |t| <= 0.25 (through t^11 and t^12; below
+// 3e-18), the library sincos beyond.  The short series is the common case:
+// with it the 256^3 FP64 real-time step (dt = 4e-4, g = 200) measured 0.817
+// -> 0.815 ms on B200.
 __device__ __forceinline__ double2 expi_small(double t) {
    if (fabs(t) > 0.25) {
       double sn, cs;
@@ -294,6 +297,15 @@ __device__ __forceinline__ double2 expi_small(double t) {
    constexpr double s3 = 1. / 6, s5 = s3 / 20, s7 = s5 / 42, s9 = s7 / 72, s11 = s9 / 110;
    constexpr double c2 = 1. / 2, c4 = c2 / 12, c6 = c4 / 30, c8 = c6 / 56, c10 = c8 / 90, c12 = c10 / 132;
    const double t2 = t * t;
+   if (fabs(t) <= 0.03125) {
+      double sq = fma(-s7, t2, s5);
+      sq = fma(sq, t2, -s3);
+      const double sn = fma(sq * t2, t, t);
+      double cq = fma(-c6, t2, c4);
+      cq = fma(cq, t2, -c2);
+      const double cs = fma(cq, t2, 1.);
+      return make_double2(cs, -sn);
+   }
    double sp = fma(-s11, t2, s9);
    sp = fma(sp, t2, -s7);
    sp = fma(sp, t2, s5);
